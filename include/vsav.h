@@ -1,0 +1,152 @@
+/* libvsav -- B200 (sm_100a) pseudo-spectral SAV time step for the vesicle
+ * growth/shrinkage model of Forstylime/Julia-Vesicles-growth-and-shrinkage.
+ *
+ * C ABI: plain pointers and sizes.  Every array argument is float64 (complex
+ * = interleaved re,im) in C order with x fastest, which is the memory order
+ * of the reference's column-major Julia arrays:
+ *   phi, psi, mu, nu        Julia (Nx,Ny[,Nz],N)      -> [V][Nz][Ny][Nx]
+ *   phi_hat ... nu_hat      Julia (Nx÷2+1,Ny[,Nz],N)  -> [V][Nz][Ny][Nx/2+1] complex
+ *   u / u_hat               Julia (Nx,Ny[,Nz],nd)     -> [R][nd][Nz][Ny][Nx]  (one block per run)
+ *   p / p_hat               Julia (Nx,Ny[,Nz])        -> [R][Nz][Ny][Nx]
+ * V = total vesicle fields of all runs, R = number of independent runs
+ * (R = 1 reproduces the reference; Nz = 1 in 2D).
+ * Host or device pointers are both accepted where data is copied in or out.
+ * All functions return 0 on success or a negative VSAV_E_* code; the text of
+ * the last error of a handle is returned by vsav_last_error().
+ * One handle = one CUDA stream; a handle is not thread safe.
+ */
+#ifndef VSAV_H
+#define VSAV_H
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VSAV_OK 0
+#define VSAV_E_INVALID (-1)       /* bad argument or unsupported size */
+#define VSAV_E_CUDA (-2)          /* CUDA runtime error (text in vsav_last_error) */
+#define VSAV_E_WC_NEGATIVE (-3)   /* W_i + C_i < 0 (Utils.jl:162,180,188 "FATAL: W+C<0") */
+#define VSAV_E_NONFINITE (-4)     /* NaN/Inf in the SAV scalars */
+#define VSAV_W_NOT_CONVERGED 1    /* psi BiCGSTAB hit itmax (Solvers.jl:76 @warn); result still valid */
+
+typedef struct vsav_handle vsav_handle;
+
+/* Config (src/Types.jl:27-134, src/Types_3d.jl:27-140).  Fields the reference
+ * types as Int (gamma_area, gamma_in, beta_in, gamma_out, beta_out, lamda) are
+ * taken as double.  psi_in_v/psi_out_v have one entry per vesicle field (V). */
+typedef struct vsav_config {
+  int32_t ndim;                 /* 2 or 3 */
+  int32_t Nx, Ny, Nz;           /* powers of two; Nz ignored in 2D */
+  int32_t N;                    /* vesicle fields per run when n_runs == 1 */
+  double epsilon, M_phi, M0_psi, eta;
+  double gamma_surf, gamma_area, gamma_bend;
+  double gamma_in, beta_in, gamma_out, beta_out, lamda;
+  double S1, S2, S3, S4, C1, C2, C3;
+  double dt, T;
+  double Lx, Ly, Lz;
+  double tol;
+  const double* psi_in_v;       /* [V] */
+  const double* psi_out_v;      /* [V] */
+} vsav_config;
+
+#define VSAV_FP64 0             /* every field and transform in FP64 */
+#define VSAV_FP32 1             /* FP32 fields/FFTs; FP64 SAV inner products, 3x3 and Q solves */
+#define VSAV_PSI_FULL 0         /* psi BiCGSTAB on full complex spectra: the reference's form */
+#define VSAV_PSI_HALF 1         /* psi BiCGSTAB on half spectra of real fields (Nyquist-projected) */
+
+typedef struct vsav_options {
+  int32_t precision;            /* VSAV_FP64 | VSAV_FP32 */
+  int32_t psi_form;             /* VSAV_PSI_FULL | VSAV_PSI_HALF */
+  int32_t psi_precond;          /* 0 = diagonal spectral (Solvers.jl:57) */
+  int32_t psi_itmax;            /* Solvers.jl:75 uses 20 */
+  double psi_rtol;              /* Solvers.jl:75 uses conf.tol */
+  double psi_atol;              /* Solvers.jl:74 uses 1e-14 */
+  int32_t n_runs;               /* R >= 1 */
+  const int32_t* run_sizes;     /* [R] vesicle fields per run (NULL: R == 1 with N fields) */
+  int32_t device;               /* CUDA device ordinal */
+} vsav_options;
+
+/* field ids (FieldState, src/Types.jl:167-201) */
+enum {
+  VSAV_PHI = 0, VSAV_PHI_HAT, VSAV_PSI, VSAV_PSI_HAT, VSAV_U, VSAV_U_HAT,
+  VSAV_P, VSAV_P_HAT, VSAV_MU, VSAV_MU_HAT, VSAV_NU, VSAV_NU_HAT
+};
+#define VSAV_PRESENT 0
+#define VSAV_OLD 1
+
+typedef struct vsav_status {
+  int32_t err_flags;            /* bit0: W1+C1<0, bit1: W2+C2<0, bit2: W3+C3<0 */
+  int32_t psi_systems;          /* BiCGSTAB systems solved in the last Step 1 (3 per run) */
+  int32_t psi_max_iters;
+  int32_t psi_not_converged;
+} vsav_status;
+
+/* build_operators(cfg) (SpectralUtils.jl:36-118) + the FieldState/Step1Cache
+ * allocations: everything on the device. */
+int vsav_create(const vsav_config* cfg, const vsav_options* opt, vsav_handle** out);
+int vsav_destroy(vsav_handle* h);
+const char* vsav_last_error(const vsav_handle* h);
+/* text of the last failed vsav_create on this thread */
+const char* vsav_create_error(void);
+/* defaults for vsav_options (FP64, FULL psi, reference BiCGSTAB settings) */
+void vsav_default_options(vsav_options* opt, const vsav_config* cfg);
+
+/* FieldState upload/download (Types.jl:167-201), level VSAV_PRESENT / VSAV_OLD */
+int vsav_set_field(vsav_handle* h, int32_t level, int32_t field, const double* data);
+int vsav_get_field(vsav_handle* h, int32_t level, int32_t field, double* data);
+/* scalars Q, R1, R2, R3 per run: q4[R][4] */
+int vsav_set_scalars(vsav_handle* h, int32_t level, const double* q4);
+int vsav_get_scalars(vsav_handle* h, int32_t level, double* q4);
+/* present.dt per run (simulation.jl:73) */
+int vsav_set_dt(vsav_handle* h, const double* dt);
+/* present.A0 per vesicle field */
+int vsav_set_A0(vsav_handle* h, const double* A0);
+int vsav_get_A0(vsav_handle* h, double* A0);
+
+/* simulation.jl:22-53: hats of phi/psi/u/p from the physical fields (unless
+ * hats_given), A0 = calculate_area(phi), R_i = sqrt(W_i + C_i), Q = 1, initial
+ * mu/nu, old = deepcopy(present). */
+int vsav_init_state(vsav_handle* h, int32_t hats_given);
+
+/* solve_step1..7 (Solvers.jl:14,144,242,267,344,431,459); n is the step index
+ * of simulation.jl:71 (n == 1 -> BDF1, else BDF2).  Results stay on the device
+ * (Step1Cache and the step intermediates); read them with vsav_get_work. */
+int vsav_step1(vsav_handle* h, int32_t n, vsav_status* st);
+int vsav_step2(vsav_handle* h, int32_t n);
+int vsav_step3(vsav_handle* h);
+int vsav_step4(vsav_handle* h, int32_t n);
+int vsav_step5(vsav_handle* h, int32_t n);
+int vsav_step6(vsav_handle* h);
+int vsav_step7(vsav_handle* h, int32_t n);
+/* update_state!(old, present) + new present from Steps 6/7 + 6 irffts (simulation.jl:88-110) */
+int vsav_update_state(vsav_handle* h);
+/* nsteps full time steps (simulation.jl:71-110) starting at step index n0 with
+ * dt[k*R + r] for step k, run r (NULL: keep the current dt).  If energy /
+ * area_ratio are non-NULL the monitor of simulation.jl:146-148 runs after every
+ * step and writes [nsteps][R]. */
+int vsav_run(vsav_handle* h, int32_t n0, int32_t nsteps, const double* dt, double* energy,
+             double* area_ratio, vsav_status* st);
+/* compute_modified_energy(present, old) and the area ratio (simulation.jl:146-147), per run */
+int vsav_monitor(vsav_handle* h, double* energy, double* area_ratio);
+
+/* intermediates: what 0 Step1Cache field (idx 0..15 in the order phi11 phi12
+ * phi13 phi14 phi21 psi11 psi12 psi21 mu11 mu12 mu13 mu14 mu21 nu11 nu12 nu21),
+ * 1 Step 3 field (phi1 psi1 phi2 psi2 mu1 nu1 mu2 nu2), 2 u_tilde_hat (idx 0/1,
+ * [R][nd][..][nkx]), 3 u_tilde physical (idx 0/1), 4 H1,H2,H3,MG physical. */
+int vsav_get_work(vsav_handle* h, int32_t what, int32_t idx, double* out);
+/* scalar intermediates: 0 Step 2 R values [R][6] (R11 R21 R31 R12 R22 R32),
+ * 1 Q [R], 2 theta_1/theta_2 [R][2], 3 area [V], 4 M_max [R],
+ * 5 psi BiCGSTAB per system [3R][4] (iters, solved, status, rnorm/eps) */
+int vsav_get_scalar_work(vsav_handle* h, int32_t what, double* out);
+
+/* to_spectral! / to_physical! (SpectralUtils.jl:132-148) on nf fields:
+ * kind 0 rfft, 1 irfft, 10+m irfft of multiplier m * input
+ * (m: 1 D1x, 2 D1y, 3 D1z, 4 Laplacian, 5 Biharmonic).  nf <= 3 V. */
+int vsav_transform(vsav_handle* h, int32_t kind, int32_t nf, const double* in, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,423 @@
+// The 2D psi solve of Step 1 (src/Solvers.jl:39-81):
+//   A x = (a/dt) x - sum_d i k_d F( M_psi F^-1( i k_d S4 x ) )
+//   preconditioner P^-1 = 1 / (a/dt - M_max S4 Laplacian)
+// solved by BiCGSTAB with Krylov.jl 0.10.6 semantics (left preconditioner by
+// multiplication, shadow vector c = b, x0 = 0, stop on ||M^-1 r|| <= atol +
+// rtol ||M^-1 b|| or itmax).  All three right-hand sides of a step (splits
+// 11, 12, 21) and every run of an ensemble are solved together: a "system" is
+// (split j, run r); its vector spans the vesicle fields of run r.
+//
+// Two formulations:
+//  FULL  the reference's own: full complex spectra [F][Ny][Nx] with the
+//        fftfreq kx0 (Nyquist negative), complex Krylov scalars, solution
+//        truncated to the half spectrum (Solvers.jl:79);
+//  HALF  the operator restricted to real fields, held as half spectra
+//        [F][Ny][kp]: the kx=0 and kx=Nx/2 columns are kept Hermitian
+//        (projection), the x derivative at kx=Nx/2 is zero (in the operator
+//        and in its preconditioner), inner products are the real
+//        Parseval-weighted ones, so the scalars are real.  It moves half the
+//        bytes of FULL but is NOT the reference's solve: FULL's Nyquist
+//        multipliers feed an anti-Hermitian (imaginary-field) channel that the
+//        truncation of Solvers.jl:79 keeps, and HALF drops it.  On resolved
+//        interfaces the two agree closely; on under-resolved ones they differ
+//        by up to ~1e-2, so FULL is the default in both precisions.
+#pragma once
+#include "kernels.cuh"
+
+namespace vsav {
+
+struct BiState {
+  double2 rho, alpha, omega, beta;
+  double rnorm, eps;
+  int iters, active, solved, status;   // status: 0 running, 1 solved, 2 itmax, 3 breakdown, 4 zero rhs
+};
+
+struct SysMap {
+  int V, R;
+  const int* run_of;
+  __device__ __forceinline__ int sys(int field) const { return (field / V) * R + run_of[field % V]; }
+};
+
+// ---------------------------------------------------------------------------
+// fused x pass of the operator: inverse x transform -> multiply by M_psi (of
+// the row's vesicle) and `scale` -> forward x transform, in place, for rows of
+// nin consecutive field blocks (t1 | t2).  HALF rows: c2r/r2c of length Nx;
+// FULL rows: c2c of length Nx.
+// ---------------------------------------------------------------------------
+template <typename T, bool FULL>
+__global__ void __launch_bounds__(256) k_rows_mul(cplx<T>* __restrict__ t, const T* __restrict__ M, T mconst, T scale,
+                                                  int logL, int nl, long long nrows, int rowlen_c, int rows_per_field,
+                                                  SysMap sm, const int* __restrict__ active, const cplx<T>* __restrict__ tab) {
+  using C = cplx<T>;
+  constexpr int E = FFTCfg<T>::E;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* s = reinterpret_cast<C*>(smraw);
+  const int L = 1 << logL, LP = line_pitch(L);
+  C* sN = s + nl * LP;
+  const long long row0 = (long long)blockIdx.x * nl;
+  const int field = (int)(row0 / rows_per_field);
+  if (active && !active[sm.sys(field % (3 * sm.V))]) return;
+  const int v = field % sm.V;
+  const int nthr = blockDim.x;
+  const int Nx = FULL ? L : 2 * L;
+  // load
+  if (FULL) {
+    for (int f = threadIdx.x; f < nl * L; f += nthr) {
+      int line = f >> logL, e = f & (L - 1);
+      if (row0 + line >= nrows) continue;
+      s[sidx(line, LP, e)] = t[(row0 + line) * rowlen_c + e];
+    }
+  } else {
+    for (int f = threadIdx.x; f < nl * (L + 1); f += nthr) {
+      int line = f / (L + 1), k = f - line * (L + 1);
+      if (row0 + line >= nrows) continue;
+      C x = t[(row0 + line) * rowlen_c + k];
+      if (k == 0 || k == L) x.y = (T)0;
+      if (k == L) sN[line] = x; else s[sidx(line, LP, k)] = x;
+    }
+    __syncthreads();
+    const int half = L / 2 + 1;
+    for (int f = threadIdx.x; f < nl * half; f += nthr) {
+      int line = f / half, k = f - line * half;
+      C A = s[sidx(line, LP, k)];
+      C B = (k == 0) ? sN[line] : s[sidx(line, LP, L - k)];
+      C w = __ldg(&tab[2 * L + k]);
+      C Zk, ZLk;
+      c2r_pre(A, B, w, Zk, ZLk);
+      s[sidx(line, LP, k)] = Zk;
+      if (k != 0 && k != L - k) s[sidx(line, LP, L - k)] = ZLk;
+    }
+  }
+  __syncthreads();
+  smem_fft<E, true>(s, LP, logL, nl, tab);
+  // multiply by M (real field) -- in HALF mode element z[m] holds x[2m] + i x[2m+1]
+  const long long prow0 = (long long)v * rows_per_field + (row0 % rows_per_field);
+  for (int f = threadIdx.x; f < nl * L; f += nthr) {
+    int line = f >> logL, e = f & (L - 1);
+    if (row0 + line >= nrows) continue;
+    const T* Mr = M ? M + (prow0 + line) * (long long)Nx : nullptr;
+    C z = s[sidx(line, LP, e)];
+    if (FULL) {
+      T m = (Mr ? Mr[e] : mconst) * scale;
+      z.x *= m; z.y *= m;
+    } else {
+      T m0 = (Mr ? Mr[2 * e] : mconst) * scale, m1 = (Mr ? Mr[2 * e + 1] : mconst) * scale;
+      z.x *= m0; z.y *= m1;
+    }
+    s[sidx(line, LP, e)] = z;
+  }
+  __syncthreads();
+  smem_fft<E, false>(s, LP, logL, nl, tab);
+  if (FULL) {
+    for (int f = threadIdx.x; f < nl * L; f += nthr) {
+      int line = f >> logL, e = f & (L - 1);
+      if (row0 + line >= nrows) continue;
+      t[(row0 + line) * rowlen_c + e] = s[sidx(line, LP, e)];
+    }
+  } else {
+    const int half = L / 2 + 1;
+    for (int f = threadIdx.x; f < nl * half; f += nthr) {
+      int line = f / half, k = f - line * half;
+      if (row0 + line >= nrows) continue;
+      C Zk = s[sidx(line, LP, k)];
+      C Zc = s[sidx(line, LP, (L - k) & (L - 1))];
+      C w = __ldg(&tab[2 * L + k]);
+      C Xk, XLk;
+      r2c_post(Zk, Zc, w, Xk, XLk);
+      C* orow = t + (row0 + line) * rowlen_c;
+      orow[k] = Xk;
+      if (k != L - k) orow[L - k] = XLk;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// wavenumbers of a vector slot (HALF: [Ny][kp] with rfftfreq kx; FULL: [Ny][Nx] fftfreq kx0)
+// ---------------------------------------------------------------------------
+struct VGeom {
+  int full;         // 1 = FULL
+  int Nx, Ny, kp, nkx;
+  long long n;      // slots per field
+  double kxs, kys;
+};
+__device__ __forceinline__ void vk(const VGeom& g, long long s, int& kx, int& ky, double& kxv, double& kyv, double& w) {
+  int rl = g.full ? g.Nx : g.kp;
+  kx = (int)(s % rl);
+  ky = (int)(s / rl);
+  kyv = kfreq(ky, g.Ny) * g.kys;
+  if (g.full) { kxv = kfreq(kx, g.Nx) * g.kxs; w = 1.0; }
+  else {
+    kxv = kx * g.kxs;
+    w = (kx >= g.nkx) ? 0.0 : ((kx == 0 || kx == g.Nx / 2) ? 1.0 : 2.0);
+  }
+}
+
+// y = a_dt * x - ( m_x t1 + i ky t2 ) at slot s of field f (HALF: Nyquist x multiplier zero)
+template <typename T>
+__device__ __forceinline__ double2 op_out(const VGeom& g, const cplx<T>* x, const cplx<T>* t1, const cplx<T>* t2,
+                                          long long j, int kx, double kxv, double kyv, double adt, double sgn) {
+  cplx<T> xv = x ? x[j] : cplx<T>{}, a = t1[j], b = t2[j];
+  double mx = (!g.full && kx == g.Nx / 2) ? 0.0 : kxv;
+  double2 d = make_double2(-(mx * (double)a.y + kyv * (double)b.y), mx * (double)a.x + kyv * (double)b.x);
+  return make_double2(adt * (double)xv.x + sgn * d.x, adt * (double)xv.y + sgn * d.y);
+}
+
+// Operator output + preconditioner + inner products.
+//   y = P^-1 ( a_dt x - (i kx t1 + i ky t2) )   (diag P^-1 = 1/(a_dt + Mmax S4 k^2); identity if !precond)
+//   HALF: the kx=0 and kx=Nx/2 columns of the operator output are made Hermitian.
+//   dots (per field): K = ndot complex (u_k^H w_k) with (u_k, w_k) from {c, y, s} ...
+//   mode 0: out y; dots <c, y>                              (q = A p; v = M^-1 q)
+//   mode 1: out y; dots <y, s>, <y, y>                      (t = M^-1 A s)
+template <typename T>
+__global__ void __launch_bounds__(256) k_psi_combine(const cplx<T>* __restrict__ x, const cplx<T>* __restrict__ t1,
+                                                     const cplx<T>* __restrict__ t2, cplx<T>* __restrict__ y,
+                                                     const cplx<T>* __restrict__ cvec, const cplx<T>* __restrict__ svec,
+                                                     int mode, const double* __restrict__ adt_r, const double* __restrict__ mmax_r,
+                                                     double S4, VGeom g, SysMap sm, const int* __restrict__ active,
+                                                     EW ew, double2* part) {
+  __shared__ double smm[2 * 4 * 8];
+  KSum acc[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+  const int f = blockIdx.y;
+  const int sy = sm.sys(f);
+  const int r = sm.run_of[f % sm.V];
+  const bool act = !active || active[sy];
+  if (act) {
+    const double adt = adt_r[r], mm = mmax_r ? mmax_r[r] : 0.0;
+    const long long beg = (long long)blockIdx.x * ew.chunk, end = min(ew.n, beg + ew.chunk);
+    for (long long s = beg + threadIdx.x; s < end; s += blockDim.x) {
+      int kx, ky; double kxv, kyv, w;
+      vk(g, s, kx, ky, kxv, kyv, w);
+      if (w == 0.0) continue;
+      long long j = (long long)f * g.n + s;
+      double2 o = op_out<T>(g, x, t1, t2, j, kx, kxv, kyv, adt, -1.0);
+      if (!g.full && (kx == 0 || kx == g.Nx / 2)) {
+        int kym = (g.Ny - ky) % g.Ny;
+        long long jm = (long long)f * g.n + (long long)kym * g.kp + kx;
+        double2 om = op_out<T>(g, x, t1, t2, jm, kx, kxv, kfreq(kym, g.Ny) * g.kys, adt, -1.0);
+        o = make_double2(0.5 * (o.x + om.x), 0.5 * (o.y - om.y));
+      }
+      if (mmax_r) {
+        // 1/(a_dt - M_max Lap S4); HALF drops the x derivative at kx = Nx/2, so does its preconditioner
+        double kxp = (!g.full && kx == g.Nx / 2) ? 0.0 : kxv;
+        double pinv = 1.0 / (adt + mm * S4 * (kxp * kxp + kyv * kyv));
+        o = make_double2(o.x * pinv, o.y * pinv);
+      }
+      cplx<T> ot; ot.x = o.x; ot.y = o.y;
+      y[j] = ot;
+      double ox = ot.x, oy = ot.y;   // use the stored (rounded) values in the dots
+      if (mode == 0) {
+        cplx<T> c = cvec[j];
+        acc[0].add(w * ((double)c.x * ox + (double)c.y * oy));
+        if (g.full) acc[1].add((double)c.x * oy - (double)c.y * ox);
+      } else {
+        cplx<T> sv = svec[j];
+        acc[0].add(w * (ox * (double)sv.x + oy * (double)sv.y));
+        if (g.full) acc[1].add(ox * (double)sv.y - oy * (double)sv.x);
+        acc[2].add(w * (ox * ox + oy * oy));
+      }
+    }
+  }
+  block_reduce_store<4>(acc, part + ((long long)blockIdx.y * ew.bpf + blockIdx.x) * 4, smm);
+}
+
+// r = M^-1 b, x = 0, p = r, dots <b, r>, ||r||^2  (Krylov.jl bicgstab initialisation)
+template <typename T>
+__global__ void __launch_bounds__(256) k_psi_init(const cplx<T>* __restrict__ b, cplx<T>* __restrict__ x, cplx<T>* __restrict__ r,
+                                                  cplx<T>* __restrict__ p, const double* __restrict__ adt_r,
+                                                  const double* __restrict__ mmax_r, double S4, VGeom g, SysMap sm,
+                                                  EW ew, double2* part) {
+  __shared__ double smm[2 * 4 * 8];
+  KSum acc[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+  const int f = blockIdx.y;
+  const int rr = sm.run_of[f % sm.V];
+  const double adt = adt_r[rr], mm = mmax_r ? mmax_r[rr] : 0.0;
+  const long long beg = (long long)blockIdx.x * ew.chunk, end = min(ew.n, beg + ew.chunk);
+  for (long long s = beg + threadIdx.x; s < end; s += blockDim.x) {
+    int kx, ky; double kxv, kyv, w;
+    vk(g, s, kx, ky, kxv, kyv, w);
+    long long j = (long long)f * g.n + s;
+    cplx<T> z{};
+    x[j] = z;
+    if (w == 0.0) { r[j] = z; p[j] = z; continue; }
+    cplx<T> bv = b[j];
+    double kxp = (!g.full && kx == g.Nx / 2) ? 0.0 : kxv;
+    double pinv = mmax_r ? 1.0 / (adt + mm * S4 * (kxp * kxp + kyv * kyv)) : 1.0;
+    cplx<T> rv; rv.x = (double)bv.x * pinv; rv.y = (double)bv.y * pinv;
+    r[j] = rv; p[j] = rv;
+    acc[0].add(w * ((double)bv.x * (double)rv.x + (double)bv.y * (double)rv.y));
+    if (g.full) acc[1].add((double)bv.x * (double)rv.y - (double)bv.y * (double)rv.x);
+    acc[2].add(w * ((double)rv.x * (double)rv.x + (double)rv.y * (double)rv.y));
+  }
+  block_reduce_store<4>(acc, part + ((long long)blockIdx.y * ew.bpf + blockIdx.x) * 4, smm);
+}
+
+// s = r - alpha v
+template <typename T>
+__global__ void k_psi_s(const cplx<T>* __restrict__ r, const cplx<T>* __restrict__ v, cplx<T>* __restrict__ s,
+                        const BiState* __restrict__ st, SysMap sm, long long n, int F) {
+  const long long tot = n * F;
+  K_LOOP(tot, i) {
+    int f = (int)(i / n);
+    const BiState& b = st[sm.sys(f)];
+    if (!b.active) continue;
+    double2 a = b.alpha;
+    cplx<T> rv = r[i], vv = v[i];
+    cplx<T> o;
+    o.x = (double)rv.x - (a.x * (double)vv.x - a.y * (double)vv.y);
+    o.y = (double)rv.y - (a.x * (double)vv.y + a.y * (double)vv.x);
+    s[i] = o;
+  }
+}
+
+// x = (x + alpha p) + omega s ;  r = s - omega t ; dots <c, r>, ||r||^2
+template <typename T>
+__global__ void __launch_bounds__(256) k_psi_update(cplx<T>* __restrict__ x, cplx<T>* __restrict__ r, const cplx<T>* __restrict__ p,
+                                                    const cplx<T>* __restrict__ s, const cplx<T>* __restrict__ t,
+                                                    const cplx<T>* __restrict__ cvec, const BiState* __restrict__ st,
+                                                    VGeom g, SysMap sm, EW ew, double2* part) {
+  __shared__ double smm[2 * 4 * 8];
+  KSum acc[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+  const int f = blockIdx.y;
+  const BiState& b = st[sm.sys(f)];
+  if (b.active) {
+    const double2 al = b.alpha, om = b.omega;
+    const long long beg = (long long)blockIdx.x * ew.chunk, end = min(ew.n, beg + ew.chunk);
+    for (long long q = beg + threadIdx.x; q < end; q += blockDim.x) {
+      int kx, ky; double kxv, kyv, w;
+      vk(g, q, kx, ky, kxv, kyv, w);
+      if (w == 0.0) continue;
+      long long j = (long long)f * g.n + q;
+      cplx<T> xv = x[j], pv = p[j], sv = s[j], tv = t[j];
+      cplx<T> xa;
+      xa.x = (double)xv.x + (al.x * (double)pv.x - al.y * (double)pv.y);
+      xa.y = (double)xv.y + (al.x * (double)pv.y + al.y * (double)pv.x);
+      cplx<T> xn;
+      xn.x = (double)xa.x + (om.x * (double)sv.x - om.y * (double)sv.y);
+      xn.y = (double)xa.y + (om.x * (double)sv.y + om.y * (double)sv.x);
+      x[j] = xn;
+      cplx<T> rn;
+      rn.x = (double)sv.x - (om.x * (double)tv.x - om.y * (double)tv.y);
+      rn.y = (double)sv.y - (om.x * (double)tv.y + om.y * (double)tv.x);
+      r[j] = rn;
+      cplx<T> c = cvec[j];
+      acc[0].add(w * ((double)c.x * (double)rn.x + (double)c.y * (double)rn.y));
+      if (g.full) acc[1].add((double)c.x * (double)rn.y - (double)c.y * (double)rn.x);
+      acc[2].add(w * ((double)rn.x * (double)rn.x + (double)rn.y * (double)rn.y));
+    }
+  }
+  block_reduce_store<4>(acc, part + ((long long)blockIdx.y * ew.bpf + blockIdx.x) * 4, smm);
+}
+
+// p = r + beta (p - omega v)   (only systems that were active in this iteration: flag `upd`)
+template <typename T>
+__global__ void k_psi_p(cplx<T>* __restrict__ p, const cplx<T>* __restrict__ r, const cplx<T>* __restrict__ v,
+                        const BiState* __restrict__ st, const int* __restrict__ upd, SysMap sm, long long n, int F) {
+  const long long tot = n * F;
+  K_LOOP(tot, i) {
+    int f = (int)(i / n);
+    int sy = sm.sys(f);
+    if (!upd[sy]) continue;
+    const BiState& b = st[sy];
+    double2 be = b.beta, om = b.omega;
+    cplx<T> pv = p[i], rv = r[i], vv = v[i];
+    double ax = (double)pv.x - (om.x * (double)vv.x - om.y * (double)vv.y);
+    double ay = (double)pv.y - (om.x * (double)vv.y + om.y * (double)vv.x);
+    cplx<T> o;
+    o.x = (double)rv.x + (be.x * ax - be.y * ay);
+    o.y = (double)rv.y + (be.x * ay + be.y * ax);
+    p[i] = o;
+  }
+}
+
+__device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
+  double d = b.x * b.x + b.y * b.y;
+  return make_double2((a.x * b.x + a.y * b.y) / d, (a.y * b.x - a.x * b.y) / d);
+}
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+
+// sums per system of per-field dot totals fd[f*4 + 0..3]
+__device__ __forceinline__ void sys_sums(const double* fd, int sy, const SysMap& sm, int F, double out[4]) {
+  out[0] = out[1] = out[2] = out[3] = 0.0;
+  int j = sy / sm.R, r = sy % sm.R;
+  for (int v = 0; v < sm.V; ++v) {
+    if (sm.run_of[v] != r) continue;
+    int f = j * sm.V + v;
+    for (int k = 0; k < 4; ++k) out[k] += fd[f * 4 + k];
+  }
+}
+
+__global__ void k_bi_init(const double* __restrict__ fd, BiState* __restrict__ st, int* __restrict__ upd, SysMap sm, int S, int F,
+                          double atol, double rtol, int itmax) {
+  int sy = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sy >= S) return;
+  double d[4];
+  sys_sums(fd, sy, sm, F, d);
+  BiState b{};
+  b.rnorm = sqrt(d[2]);
+  b.eps = atol + rtol * b.rnorm;
+  b.rho = make_double2(d[0], d[1]);
+  b.alpha = b.omega = make_double2(1.0, 0.0);
+  b.iters = 0;
+  if (b.rnorm == 0.0) { b.solved = 1; b.status = 4; b.active = 0; }
+  else if (b.rho.x == 0.0 && b.rho.y == 0.0) { b.solved = 0; b.status = 3; b.active = 0; }
+  else {
+    b.solved = b.rnorm <= b.eps;
+    b.active = !(b.solved || itmax <= 0);
+    b.status = b.solved ? 1 : (b.active ? 0 : 2);
+  }
+  st[sy] = b;
+  upd[sy] = b.active;
+}
+__global__ void k_bi_alpha(const double* __restrict__ fd, BiState* __restrict__ st, SysMap sm, int S, int F) {
+  int sy = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sy >= S || !st[sy].active) return;
+  double d[4];
+  sys_sums(fd, sy, sm, F, d);
+  st[sy].alpha = cdiv(st[sy].rho, make_double2(d[0], d[1]));
+}
+__global__ void k_bi_omega(const double* __restrict__ fd, BiState* __restrict__ st, SysMap sm, int S, int F) {
+  int sy = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sy >= S || !st[sy].active) return;
+  double d[4];
+  sys_sums(fd, sy, sm, F, d);
+  st[sy].omega = cdiv(make_double2(d[0], d[1]), make_double2(d[2], 0.0));
+}
+__global__ void k_bi_beta(const double* __restrict__ fd, BiState* __restrict__ st, int* __restrict__ upd, SysMap sm, int S, int F,
+                          int itmax, int* __restrict__ any_active) {
+  int sy = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sy >= S) return;
+  BiState b = st[sy];
+  upd[sy] = b.active;
+  if (!b.active) return;
+  double d[4];
+  sys_sums(fd, sy, sm, F, d);
+  double2 nr = make_double2(d[0], d[1]);
+  b.beta = cmul(cdiv(nr, b.rho), cdiv(b.alpha, b.omega));
+  b.rho = nr;
+  b.rnorm = sqrt(d[2]);
+  b.iters += 1;
+  bool mach = (b.rnorm + 1.0 <= 1.0);
+  bool solved = (b.rnorm <= b.eps) || mach;
+  bool tired = b.iters >= itmax;
+  bool brk = (b.alpha.x == 0.0 && b.alpha.y == 0.0) || isnan(b.alpha.x) || isnan(b.alpha.y);
+  b.solved = solved;
+  b.active = !(solved || tired || brk);
+  b.status = solved ? 1 : (brk ? 3 : (tired ? 2 : 0));
+  st[sy] = b;
+  if (b.active) atomicOr(any_active, 1);
+}
+
+// full -> half truncation of the solution (Solvers.jl:79):  half[f][y][kx] = full[f][y][kx], kx < nkx
+template <typename T>
+__global__ void k_trunc(const cplx<T>* __restrict__ full, cplx<T>* __restrict__ half, int Nx, int Ny, int kp, int nkx, int F) {
+  long long tot = (long long)F * Ny * kp;
+  K_LOOP(tot, i) {
+    int kx = (int)(i % kp);
+    long long row = i / kp;
+    cplx<T> z{};
+    if (kx < nkx) z = full[row * Nx + kx];
+    half[i] = z;
+  }
+}
+
+}  // namespace vsav

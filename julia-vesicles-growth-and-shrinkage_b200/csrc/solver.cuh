@@ -1,0 +1,791 @@
+// Host orchestration of one SAV time step on the device: the analogue of
+// Operators (src/Types.jl:298-342) + solve_step1..7 (src/Solvers.jl) + the
+// loop body of run_simulation (src/simulation.jl:71-148).
+//
+// All state lives on the device.  Two time levels (present, old) are swapped
+// by pointer at the end of a step, which is what update_state!
+// (src/Types.jl:243-265) achieves by copying.
+#pragma once
+#include <vector>
+#include <memory>
+#include <algorithm>
+#include "psi.cuh"
+
+namespace vsav {
+
+enum FieldId : int { F_PHI = 0, F_PHI_HAT, F_PSI, F_PSI_HAT, F_U, F_U_HAT, F_P, F_P_HAT, F_MU, F_MU_HAT, F_NU, F_NU_HAT };
+
+struct Options {
+  int precision = 0;       // 0 FP64, 1 FP32 bulk
+  int psi_form = 0;        // 0 FULL (reference form), 1 HALF
+  int psi_precond = 0;     // 0 diagonal, 1 learned (flexible)
+  int psi_itmax = 20;
+  double psi_rtol = 1e-12, psi_atol = 1e-14;
+  int check_every_iter = 1;  // read back convergence flags each BiCGSTAB iteration
+};
+
+struct StepStatus {
+  int err_flags = 0;        // 1,2,4: W_i + C_i < 0
+  int psi_systems = 0;
+  int psi_max_iters = 0;
+  int psi_not_converged = 0;
+  double psi_max_rnorm_rel = 0.0;
+};
+
+class SolverBase {
+ public:
+  virtual ~SolverBase() {}
+  virtual void set_field(int level, int fid, const void* host, int is_device) = 0;
+  virtual void get_field(int level, int fid, void* host) = 0;
+  virtual void set_scalars(int level, const double* q4 /* [R][4] Q,R1,R2,R3 */) = 0;
+  virtual void get_scalars(int level, double* q4) = 0;
+  virtual void set_dt(const double* dt) = 0;
+  virtual void get_dt(double* dt) = 0;
+  virtual void set_A0(const double* a0) = 0;
+  virtual void get_A0(double* a0) = 0;
+  virtual void init_state(int hats_given) = 0;
+  virtual void step1(int n) = 0;
+  virtual void step2(int n) = 0;
+  virtual void step3() = 0;
+  virtual void step4(int n) = 0;
+  virtual void step5(int n) = 0;
+  virtual void step6() = 0;
+  virtual void step7(int n) = 0;
+  virtual void update_state() = 0;
+  virtual void monitor(double* energy, double* aratio) = 0;
+  virtual void get_work(int what, int idx, void* host) = 0;
+  virtual void get_scalar_work(int what, double* out) = 0;
+  virtual void transform(int kind, int nf, const double* in, double* out) = 0;
+  virtual StepStatus status() = 0;
+  virtual void sync() = 0;
+};
+
+struct Dims {
+  int nd, Nx, Ny, Nz, V, R;
+  double Lx, Ly, Lz;
+};
+
+__global__ void k_copy_mmax(const double* sch, double* mm, int R) {
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < R) mm[r] = sch[r * 8 + 3];
+  }
+
+__global__ void k_set_adt(const double* dt, double a, double* adt, int R) {
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < R) adt[r] = a / dt[r];
+  }
+
+__global__ void k_area0(const double* fd, double cell, double* A0, int V) {
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < V) A0[v] = fd[v * 3] * cell;
+  }
+
+__global__ void k_init_scalars(const double* sch, double* s, int R) {
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < R) { s[r * 4 + 0] = 1.0; s[r * 4 + 1] = sch[r * 8 + 0]; s[r * 4 + 2] = sch[r * 8 + 1]; s[r * 4 + 3] = sch[r * 8 + 2]; }
+  }
+
+__global__ void k_bi_flags(const BiState* st_, int* upd, int S) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < S) upd[s] = st_[s].active;
+  }
+
+template <typename T>
+__global__ void k_import_real(const double* src, T* dst, int Fo, int Fi, long long P, int dir) {
+    long long tot = (long long)Fo * Fi * P;
+    K_LOOP(tot, i) {
+      long long p = i % P, f = i / P;
+      int o = (int)(f / Fi), in = (int)(f % Fi);
+      long long d = ((long long)in * Fo + o) * P + p;
+      if (dir == 0) dst[d] = (T)src[i]; else ((double*)src)[i] = (double)dst[d];
+    }
+  }
+
+template <typename T>
+__global__ void k_import_hat(const double* src, cplx<T>* dst, int Fo, int Fi, long long rows, int nkx, int kp, int dir) {
+    long long tot = (long long)Fo * Fi * rows * nkx;
+    K_LOOP(tot, i) {
+      int kx = (int)(i % nkx);
+      long long rr = i / nkx;
+      long long row = rr % rows, f = rr / rows;
+      int o = (int)(f / Fi), in = (int)(f % Fi);
+      long long d = (((long long)in * Fo + o) * rows + row) * kp + kx;
+      if (dir == 0) { cplx<T> z; z.x = (T)src[2 * i]; z.y = (T)src[2 * i + 1]; dst[d] = z; }
+      else { ((double*)src)[2 * i] = (double)dst[d].x; ((double*)src)[2 * i + 1] = (double)dst[d].y; }
+    }
+  }
+
+template <typename T>
+class Solver : public SolverBase {
+ public:
+  using C = cplx<T>;
+  Geom g{};
+  Phys ph{};
+  Options opt;
+  Dims dm;
+  cudaStream_t st = nullptr;
+  std::vector<void*> allocs;
+  // device bookkeeping
+  int *d_run_of = nullptr, *d_vbeg = nullptr;
+  double *d_psi_in = nullptr, *d_psi_out = nullptr;
+  Runs rn{};
+  C* tab = nullptr;
+  // state levels
+  T* phys4[2]; C* hat4[2]; T* uphys[2]; C* uhat[2]; double* sc[2];
+  double *d_dt, *d_A0, *d_adt;
+  // step-1 work
+  T *phis, *psis, *Mpsi, *ustar, *d4, *omega, *lapomega, *H4, *gG, *gstar, *adv;
+  C *tmpH, *tmpH2, *Hh, *flh, *advh, *cache, *rhs, *s3, *uth;
+  T *cphys, *mn, *gu, *gmu, *gnu, *conv, *coupl, *rhs2, *utp, *tmpP, *mon_lap, *mon_g4, *mon_ga, *mon_gp;
+  double *scH, *factor, *area, *mmax_v, *mmax_r, *fd, *fd2, *r2, *qv, *theta, *energy, *aratio;
+  double2* part;
+  int* d_err;
+  // psi solver
+  C *vb, *vx, *vr, *vp, *vv, *vs, *vt, *vt12;
+  BiState* bst; int *bupd, *d_any;
+  int* h_pinned_any = nullptr;
+  StepStatus last;
+  double* stage = nullptr;   // host-format staging
+  size_t stage_bytes = 0;
+  double cur_a = 1, cur_b = -1, cur_c = 0;
+
+  template <typename X> X* dalloc(size_t n) {
+    void* p = nullptr;
+    VSAV_CUDA(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(X)));
+    VSAV_CUDA(cudaMemsetAsync(p, 0, std::max<size_t>(n, 1) * sizeof(X), st));
+    allocs.push_back(p);
+    return (X*)p;
+  }
+
+  static int ilog2(int n) { int l = 0; while ((1 << l) < n) ++l; return l; }
+
+  Solver(const Dims& d, const Phys& p, const Options& o, const int* run_sizes, const double* psi_in, const double* psi_out)
+      : ph(p), opt(o), dm(d) {
+    VSAV_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    g.nd = d.nd; g.Nx = d.Nx; g.Ny = d.Ny; g.Nz = (d.nd == 3) ? d.Nz : 1;
+    g.nkx = d.Nx / 2 + 1;
+    g.kp = (g.nkx + 15) / 16 * 16;
+    g.P = (long long)g.Nz * g.Ny * g.Nx;
+    g.H = (long long)g.Nz * g.Ny * g.kp;
+    g.Pfull = (long long)g.Nz * g.Ny * g.Nx;
+    g.kxs = 2 * M_PI / d.Lx; g.kys = 2 * M_PI / d.Ly; g.kzs = (d.nd == 3) ? 2 * M_PI / d.Lz : 0.0;
+    const int V = d.V, R = d.R, nd = d.nd;
+    // runs
+    std::vector<int> run_of(V), vbeg(R + 1);
+    int v = 0;
+    for (int r = 0; r < R; ++r) { vbeg[r] = v; for (int k = 0; k < run_sizes[r]; ++k) run_of[v++] = r; }
+    vbeg[R] = v;
+    if (v != V) throw std::runtime_error("run sizes do not add up to the number of vesicle fields");
+    d_run_of = dalloc<int>(V); d_vbeg = dalloc<int>(R + 1);
+    d_psi_in = dalloc<double>(V); d_psi_out = dalloc<double>(V);
+    VSAV_CUDA(cudaMemcpyAsync(d_run_of, run_of.data(), V * sizeof(int), cudaMemcpyHostToDevice, st));
+    VSAV_CUDA(cudaMemcpyAsync(d_vbeg, vbeg.data(), (R + 1) * sizeof(int), cudaMemcpyHostToDevice, st));
+    VSAV_CUDA(cudaMemcpyAsync(d_psi_in, psi_in, V * sizeof(double), cudaMemcpyHostToDevice, st));
+    VSAV_CUDA(cudaMemcpyAsync(d_psi_out, psi_out, V * sizeof(double), cudaMemcpyHostToDevice, st));
+    rn.V = V; rn.R = R; rn.run_of = d_run_of; rn.vbeg = d_vbeg; rn.psi_in = d_psi_in; rn.psi_out = d_psi_out;
+    // twiddles: tab[n + m] = exp(-2 pi i m / n), n = 1..2^k
+    int nmax = std::max(g.Nx, std::max(g.Ny, g.Nz));
+    std::vector<C> ht(2 * nmax);
+    for (int n = 1; n <= nmax; n <<= 1)
+      for (int m = 0; m < n; ++m) {
+        long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)n;
+        // exact values at the quarter points
+        long double cr = cosl(a), ci = sinl(a);
+        if (4 * m % n == 0) { int q = 4 * m / n; cr = (q == 0) ? 1 : (q == 2 ? -1 : 0); ci = (q == 1) ? -1 : (q == 3 ? 1 : 0); }
+        ht[n + m] = mk<C>((double)cr, (double)ci);
+      }
+    tab = dalloc<C>(2 * nmax);
+    VSAV_CUDA(cudaMemcpyAsync(tab, ht.data(), ht.size() * sizeof(C), cudaMemcpyHostToDevice, st));
+    VSAV_CUDA(cudaStreamSynchronize(st));
+    const long long VP = (long long)V * g.P, VH = (long long)V * g.H, RP = (long long)R * g.P, RH = (long long)R * g.H;
+    (void)VH;
+    for (int l = 0; l < 2; ++l) {
+      phys4[l] = dalloc<T>(4 * VP); hat4[l] = dalloc<C>(4 * VH);
+      uphys[l] = dalloc<T>((nd + 1) * RP); uhat[l] = dalloc<C>((nd + 1) * RH);
+      sc[l] = dalloc<double>(4 * R);
+    }
+    d_dt = dalloc<double>(R); d_A0 = dalloc<double>(V); d_adt = dalloc<double>(R);
+    phis = dalloc<T>(VP); psis = dalloc<T>(VP); Mpsi = dalloc<T>(VP); ustar = dalloc<T>(nd * RP);
+    d4 = dalloc<T>(4 * VP); omega = dalloc<T>(VP); lapomega = dalloc<T>(VP); H4 = dalloc<T>(4 * VP);
+    gG = dalloc<T>(3 * VP); gstar = dalloc<T>(2 * nd * VP); adv = dalloc<T>(2 * VP);
+    long long tmpf = std::max<long long>(8 * V, 9 * R);
+    tmpH = dalloc<C>(tmpf * g.H); tmpH2 = dalloc<C>(V * g.H); Hh = dalloc<C>(4 * VH); flh = dalloc<C>(3 * VH);
+    advh = dalloc<C>(2 * VH); cache = dalloc<C>(16 * VH); rhs = dalloc<C>(3 * VH); s3 = dalloc<C>(8 * VH);
+    uth = dalloc<C>(2 * nd * RH);
+    cphys = dalloc<T>(8 * VP); mn = dalloc<T>(4 * VP); gu = dalloc<T>(nd * nd * RP); gmu = dalloc<T>(nd * VP);
+    gnu = dalloc<T>(nd * VP); conv = dalloc<T>(nd * RP); coupl = dalloc<T>(nd * RP); rhs2 = dalloc<T>(nd * RP);
+    utp = dalloc<T>(2 * nd * RP); tmpP = dalloc<T>(3 * VP);
+    mon_lap = dalloc<T>(2 * VP); mon_g4 = dalloc<T>(4 * VP); mon_ga = dalloc<T>(2 * VP); mon_gp = dalloc<T>(2 * RP);
+    scH = dalloc<double>(8 * R); factor = dalloc<double>(V); area = dalloc<double>(V);
+    mmax_v = dalloc<double>(V); mmax_r = dalloc<double>(R);
+    fd = dalloc<double>(3 * V * 32 + R * 32); fd2 = dalloc<double>(3 * V * 32 + R * 32);
+    r2 = dalloc<double>(6 * R); qv = dalloc<double>(R); theta = dalloc<double>(2 * R);
+    energy = dalloc<double>(R); aratio = dalloc<double>(R);
+    long long nmaxe = std::max<long long>(g.Pfull, g.H);
+    long long bpf = (nmaxe + 2047) / 2048;
+    part = dalloc<double2>(bpf * std::max(3 * V, R) * 32);
+    d_err = dalloc<int>(1);
+    if (nd == 2) {
+      long long n = psi_n();
+      vb = dalloc<C>(3 * V * n); vr = dalloc<C>(3 * V * n); vp = dalloc<C>(3 * V * n);
+      vv = dalloc<C>(3 * V * n); vs = dalloc<C>(3 * V * n); vt = dalloc<C>(3 * V * n); vt12 = dalloc<C>(6 * V * n);
+      vx = psi_full() ? dalloc<C>(3 * V * n) : nullptr;
+      bst = dalloc<BiState>(3 * R); bupd = dalloc<int>(3 * R); d_any = dalloc<int>(1);
+      VSAV_CUDA(cudaMallocHost(&h_pinned_any, sizeof(int)));
+    }
+    long long nh = std::max<long long>(3LL * V, 2LL * R * nd) * std::max<long long>(g.P, (long long)g.Nz * g.Ny * g.nkx * 2);
+    stage_bytes = nh * sizeof(double);
+    stage = dalloc<double>(nh);
+    VSAV_CUDA(cudaStreamSynchronize(st));
+  }
+
+  ~Solver() override {
+    cudaStreamSynchronize(st);
+    for (void* p : allocs) cudaFree(p);
+    if (h_pinned_any) cudaFreeHost(h_pinned_any);
+    cudaStreamDestroy(st);
+  }
+
+  bool psi_full() const { return opt.psi_form == 0; }
+  long long psi_n() const { return psi_full() ? g.Pfull : g.H; }
+
+  // ------------------------------------------------------------------ launch helpers
+  EW ew(long long n) const {
+    EW e; e.n = n; e.chunk = std::min<long long>(2048, n); e.bpf = (int)((n + e.chunk - 1) / e.chunk); return e;
+  }
+  int gridfor(long long n, int bs = 256) const { long long b = (n + bs - 1) / bs; return (int)std::min<long long>(b, 148 * 16); }
+  void fin(int K, int F, const EW& e, double* out) {
+    k_fin_fields<<<F, 256, 0, st>>>(part, e.bpf, K, out);
+    VSAV_LAUNCH_CHECK();
+  }
+
+  int rows_nl(int L, long long nrows, int cap_rows_per_field = 0) const {
+    int nl = std::max(1, FFTCfg<T>::CHUNK / L);
+    while (nl > 1 && nl / 2 >= nrows) nl /= 2;
+    if (cap_rows_per_field) while (nl > cap_rows_per_field) nl /= 2;
+    return nl;
+  }
+  size_t rows_smem(int L, int nl) const { return (size_t)(nl * line_pitch(L) + nl) * sizeof(C); }
+
+  void rows_r2c(const T* in0, const T* in1, double a0, double a1, C* out, long long nrows) {
+    int L = g.Nx / 2, logL = ilog2(L);
+    int nl = rows_nl(L, nrows);
+    int thr = std::max(32, nl * L / FFTCfg<T>::E);
+    long long grid = (nrows + nl - 1) / nl;
+    k_rows_r2c<T><<<(unsigned)grid, thr, rows_smem(L, nl), st>>>(in0, in1, (T)a0, (T)a1, out, logL, nl, nrows, g.kp, tab);
+    VSAV_LAUNCH_CHECK();
+  }
+  void rows_c2r(const C* in, T* out, double scale, long long nrows) {
+    int L = g.Nx / 2, logL = ilog2(L);
+    int nl = rows_nl(L, nrows);
+    int thr = std::max(32, nl * L / FFTCfg<T>::E);
+    long long grid = (nrows + nl - 1) / nl;
+    k_rows_c2r<T><<<(unsigned)grid, thr, rows_smem(L, nl), st>>>(in, out, (T)scale, logL, nl, nrows, g.kp, tab);
+    VSAV_LAUNCH_CHECK();
+  }
+  template <bool INV>
+  void rows_c2c(const C* in, const T* in_real, C* out, double scale, long long nrows) {
+    int L = g.Nx, logL = ilog2(L);
+    int nl = rows_nl(L, nrows);
+    int thr = std::max(32, nl * L / FFTCfg<T>::E);
+    long long grid = (nrows + nl - 1) / nl;
+    k_rows_c2c<T, INV><<<(unsigned)grid, thr, rows_smem(L, nl), st>>>(in, in_real, out, (T)scale, logL, nl, nrows, tab);
+    VSAV_LAUNCH_CHECK();
+  }
+  // geo: 0 2D y (half), 1 3D z (half), 2 3D y (half), 3 2D y (full)
+  ColArgs colargs(int geo, long long& nouter) const {
+    ColArgs a{};
+    a.geo = geo; a.Nx = g.Nx; a.Ny = g.Ny; a.Nz = g.Nz; a.kp = g.kp;
+    a.kxs = g.kxs; a.kys = g.kys; a.kzs = g.kzs;
+    int L;
+    if (geo == 0) { L = g.Ny; a.S = g.kp; a.W = g.kp; a.O = (long long)g.Ny * g.kp; a.kpv = g.kp; a.nkv = g.nkx; }
+    else if (geo == 1) { L = g.Nz; a.S = g.Ny * g.kp; a.W = g.Ny * g.kp; a.O = g.H; a.kpv = g.kp; a.nkv = g.nkx; }
+    else if (geo == 2) { L = g.Ny; a.S = g.kp; a.W = g.kp; a.O = (long long)g.Ny * g.kp; a.kpv = g.kp; a.nkv = g.nkx; nouter *= g.Nz; }
+    else { L = g.Ny; a.S = g.Nx; a.W = g.Nx; a.O = (long long)g.Ny * g.Nx; a.kpv = g.Nx; a.nkv = g.Nx; }
+    a.logL = ilog2(L);
+    int TW = std::max(1, FFTCfg<T>::CHUNK / L);
+    while (TW > 1 && TW / 2 >= a.W) TW /= 2;
+    a.TW = TW;
+    a.tiles = (a.W + TW - 1) / TW;
+    return a;
+  }
+  void cols(bool inv, int geo, long long nf, const C* in0, const C* in1, double a0, double a1, int mult, double ms,
+            C* out, double oscale) {
+    long long nouter = nf;
+    ColArgs a = colargs(geo, nouter);
+    int L = 1 << a.logL;
+    int thr = std::max(32, a.TW * L / FFTCfg<T>::E);
+    size_t sm = (size_t)(a.TW * line_pitch(L)) * sizeof(C);
+    long long grid = (long long)a.tiles * nouter;
+    if (inv) k_cols<T, true><<<(unsigned)grid, thr, sm, st>>>(in0, in1, (T)a0, (T)a1, mult, ms, out, (T)oscale, a, tab);
+    else k_cols<T, false><<<(unsigned)grid, thr, sm, st>>>(in0, in1, (T)a0, (T)a1, mult, ms, out, (T)oscale, a, tab);
+    VSAV_LAUNCH_CHECK();
+  }
+  // rfft over the nd spatial axes of nf real fields  (in = a0 in0 + a1 in1)
+  void rfft(const T* in0, long long nf, C* out, const T* in1 = nullptr, double a0 = 1, double a1 = 0) {
+    rows_r2c(in0, in1, a0, a1, out, nf * g.Nz * g.Ny);
+    if (g.nd == 2) cols(false, 0, nf, out, nullptr, 1, 0, M_ONE, 1, out, 1);
+    else { cols(false, 2, nf, out, nullptr, 1, 0, M_ONE, 1, out, 1); cols(false, 1, nf, out, nullptr, 1, 0, M_ONE, 1, out, 1); }
+  }
+  // irfft of mult * (a0 in0 + a1 in1), normalised (the reference's ifft plans)
+  void irfft(const C* in0, long long nf, T* out, int mult = M_ONE, double ms = 1.0, const C* in1 = nullptr, double a0 = 1,
+             double a1 = 0) {
+    if (nf * g.H > std::max<long long>(8 * dm.V, 9 * dm.R) * g.H) throw std::runtime_error("irfft batch too large");
+    if (g.nd == 2) cols(true, 0, nf, in0, in1, a0, a1, mult, ms, tmpH, 1);
+    else { cols(true, 1, nf, in0, in1, a0, a1, mult, ms, tmpH, 1); cols(true, 2, nf, tmpH, nullptr, 1, 0, M_ONE, 1, tmpH, 1); }
+    rows_c2r(tmpH, out, 1.0 / (double)g.P, nf * g.Nz * g.Ny);
+  }
+
+  // ------------------------------------------------------------------ pieces
+  void set_bdf(int n) {
+    if (n == 1) { cur_a = 1.0; cur_b = -1.0; cur_c = 0.0; } else { cur_a = 1.5; cur_b = -2.0; cur_c = 0.5; }
+  }
+
+  // H1, H2, H3, MG at (phi, psi)  (+ W3 integrands, M_psi when phio given) -> H4, Hh, scH
+  void compute_H(const T* phi_in, const T* phio, const T* psi_in, const T* psio, bool star) {
+    const int V = dm.V;
+    const long long VP = (long long)V * g.P;
+    EW e = ew(g.P);
+    dim3 gv(e.bpf, V);
+    const T *phi = phi_in, *psi = psi_in;
+    if (star) {
+      k_star<T><<<gv, 256, 0, st>>>(phi_in, phio, psi_in, psio, phis, psis, Mpsi, ph, rn, e, part);
+      VSAV_LAUNCH_CHECK();
+      phi = phis; psi = psis;
+    } else {
+      k_star<T><<<gv, 256, 0, st>>>(phi_in, nullptr, psi_in, nullptr, nullptr, nullptr, nullptr, ph, rn, e, part);
+      VSAV_LAUNCH_CHECK();
+    }
+    fin(3, V, e, fd2);                                   // fd2[v*3+1..2] = f_osm, psi^2
+    if (star) { k_fin_max<<<V, 32, 0, st>>>(part, e.bpf, 3, 0, mmax_v); VSAV_LAUNCH_CHECK(); }
+    rfft(phi, V, tmpH2);
+    irfft(tmpH2, V, d4, M_DX);
+    irfft(tmpH2, V, d4 + VP, M_DY);
+    irfft(tmpH2, V, d4 + 2 * VP, M_LAP);
+    irfft(tmpH2, V, d4 + 3 * VP, M_BIH);
+    k_surf<T><<<gv, 256, 0, st>>>(phi, d4, d4 + VP, d4 + 2 * VP, omega, ph, e, part);
+    VSAV_LAUNCH_CHECK();
+    fin(3, V, e, fd);                                    // fd[v*3+0..2] = surf, bend, E2
+    k_fin_H<<<(dm.R + 63) / 64, 64, 0, st>>>(fd, fd2, star ? mmax_v : nullptr, d_A0, ph, rn, scH, factor, area, d_err);
+    VSAV_LAUNCH_CHECK();
+    if (star) { k_copy_mmax<<<(dm.R + 63) / 64, 64, 0, st>>>(scH, mmax_r, dm.R); VSAV_LAUNCH_CHECK(); }
+    rfft(omega, V, tmpH2);
+    irfft(tmpH2, V, lapomega, M_LAP);
+    k_H<T><<<gv, 256, 0, st>>>(phi, psi, omega, lapomega, d4 + 2 * VP, d4 + 3 * VP, scH, factor, H4, VP, ph, rn, e);
+    VSAV_LAUNCH_CHECK();
+    rfft(H4, 4LL * V, Hh);
+  }
+
+
+  // ------------------------------------------------------------------ steps
+  void step1(int n) override {
+    set_bdf(n);
+    const int V = dm.V, R = dm.R, nd = g.nd;
+    const long long VP = (long long)V * g.P, VH = (long long)V * g.H, RP = (long long)R * g.P;
+    compute_H(phys4[0], phys4[1], phys4[0] + VP, phys4[1] + VP, true);
+    k_axpby<T><<<gridfor(nd * RP), 256, 0, st>>>(uphys[0], uphys[1], ustar, 2.0, -1.0, nd * RP);
+    VSAV_LAUNCH_CHECK();
+    // psi 12 flux: D1_d . rfft(M dG/dx_d)
+    const C* Gh = Hh + 3 * VH;
+    for (int d = 0; d < nd; ++d) irfft(Gh, V, gG + d * VP, M_DX + d);
+    if (nd == 2) {
+      k_mul_field<T><<<gridfor(VP), 256, 0, st>>>(gG, Mpsi, 1.0, gG, VP, 1);
+      k_mul_field<T><<<gridfor(VP), 256, 0, st>>>(gG + VP, Mpsi, 1.0, gG + VP, VP, 1);
+    } else {
+      k_mul_field<T><<<gridfor(3 * VP), 256, 0, st>>>(gG, nullptr, ph.M0_psi, gG, 3 * VP, 1);
+    }
+    VSAV_LAUNCH_CHECK();
+    rfft(gG, (long long)nd * V, flh);
+    // advection of the stored spectra: u* . grad(phi*), u* . grad(psi*)
+    for (int q = 0; q < 2; ++q)
+      for (int d = 0; d < nd; ++d)
+        irfft(hat4[0] + q * VH, V, gstar + (q * nd + d) * VP, M_DX + d, 1.0, hat4[1] + q * VH, 2.0, -1.0);
+    k_advect<T><<<gridfor(2 * VP), 256, 0, st>>>(gstar, ustar, adv, 2, nd, rn, g.P);
+    VSAV_LAUNCH_CHECK();
+    rfft(adv, 2LL * V, advh);
+    k_set_adt<<<(R + 63) / 64, 64, 0, st>>>(d_dt, cur_a, d_adt, R);
+    k_step1_k<T><<<gridfor(VH), 256, 0, st>>>(hat4[0], hat4[1], Hh, flh, nd, advh, cache, rhs, d_dt, cur_a, cur_b, cur_c,
+                                              ph, rn, g);
+    VSAV_LAUNCH_CHECK();
+    if (nd == 2) {
+      psi_solve();
+      k_nu<T><<<gridfor(VH), 256, 0, st>>>(cache, Gh, ph.S4, VH, g);
+      VSAV_LAUNCH_CHECK();
+    }
+  }
+
+  void step2(int n) override {
+    set_bdf(n);
+    const int V = dm.V;
+    const long long VP = (long long)V * g.P;
+    irfft(cache, 8LL * V, cphys);
+    EW e = ew(g.P);
+    k_dot2<T><<<dim3(e.bpf, V), 256, 0, st>>>(H4, phys4[0], phys4[1], phys4[0] + VP, phys4[1] + VP, cphys, cur_b, cur_c, VP, e, part);
+    VSAV_LAUNCH_CHECK();
+    fin(22, V, e, fd);
+    k_fin_step2<<<(dm.R + 63) / 64, 64, 0, st>>>(fd, sc[0], sc[1], cur_a, cur_b, cur_c, ph, rn, r2);
+    VSAV_LAUNCH_CHECK();
+  }
+
+  void step3() override {
+    const long long VH = (long long)dm.V * g.H;
+    k_step3<T><<<gridfor(VH), 256, 0, st>>>(cache, r2, s3, rn, g);
+    VSAV_LAUNCH_CHECK();
+  }
+
+  void step4(int n) override {
+    set_bdf(n);
+    const int V = dm.V, R = dm.R, nd = g.nd;
+    const long long VP = (long long)V * g.P, VH = (long long)V * g.H, RP = (long long)R * g.P, RH = (long long)R * g.H;
+    for (int c = 0; c < nd; ++c)
+      for (int d = 0; d < nd; ++d)
+        irfft(uhat[0] + c * RH, R, gu + (c * nd + d) * RP, M_DX + d, 1.0, uhat[1] + c * RH, 2.0, -1.0);
+    for (int d = 0; d < nd; ++d) {
+      irfft(hat4[0] + 2 * VH, V, gmu + d * VP, M_DX + d, 1.0, hat4[1] + 2 * VH, 2.0, -1.0);
+      irfft(hat4[0] + 3 * VH, V, gnu + d * VP, M_DX + d, 1.0, hat4[1] + 3 * VH, 2.0, -1.0);
+    }
+    k_conv_coupl<T><<<gridfor(RP), 256, 0, st>>>(ustar, gu, phis, psis, gmu, gnu, conv, coupl, rhs2, ph.lamda, nd, rn, g.P);
+    VSAV_LAUNCH_CHECK();
+    rfft(rhs2, (long long)nd * R, uth + nd * RH);
+    k_step4_k<T><<<gridfor(RH), 256, 0, st>>>(uhat[0], uhat[1], uth, d_dt, cur_a, cur_b, cur_c, ph, R, g);
+    VSAV_LAUNCH_CHECK();
+    irfft(uth, 2LL * nd * R, utp);
+  }
+
+  void step5(int n) override {
+    set_bdf(n);
+    const int V = dm.V, R = dm.R;
+    const long long VP = (long long)V * g.P, VH = (long long)V * g.H, RP = (long long)R * g.P;
+    irfft(s3 + 4 * VH, 4LL * V, mn);
+    EW e = ew(g.P);
+    k_dot5v<T><<<dim3(e.bpf, V), 256, 0, st>>>(adv, mn, VP, e, part);
+    VSAV_LAUNCH_CHECK();
+    fin(4, V, e, fd);
+    k_dot5r<T><<<dim3(e.bpf, R), 256, 0, st>>>(coupl, conv, utp, g.nd, RP, e, part);
+    VSAV_LAUNCH_CHECK();
+    fin(4, R, e, fd2);
+    k_fin_step5<<<(R + 63) / 64, 64, 0, st>>>(fd, fd2, sc[0], sc[1], d_dt, g.nd == 3, cur_a, cur_b, cur_c, ph, rn, qv, theta);
+    VSAV_LAUNCH_CHECK();
+  }
+
+  void step6() override {
+    const long long VH = (long long)dm.V * g.H;
+    k_step6<T><<<gridfor(VH), 256, 0, st>>>(s3, qv, hat4[1], rn, g);
+    k_step6_scalars<<<(dm.R + 63) / 64, 64, 0, st>>>(r2, qv, sc[1], dm.R);
+    VSAV_LAUNCH_CHECK();
+  }
+
+  void step7(int n) override {
+    set_bdf(n);
+    const long long RH = (long long)dm.R * g.H;
+    k_step67<T><<<gridfor(RH), 256, 0, st>>>(uth, qv, uhat[0], uhat[1], d_dt, cur_a, ph, dm.R, g);
+    VSAV_LAUNCH_CHECK();
+  }
+
+  // old <- present ; present <- new (written into old's storage by steps 6/7) ; physical fields by irfft
+  void update_state() override {
+    std::swap(phys4[0], phys4[1]); std::swap(hat4[0], hat4[1]);
+    std::swap(uphys[0], uphys[1]); std::swap(uhat[0], uhat[1]);
+    std::swap(sc[0], sc[1]);
+    irfft(hat4[0], 4LL * dm.V, phys4[0]);
+    irfft(uhat[0], (long long)(g.nd + 1) * dm.R, uphys[0]);
+  }
+
+  void monitor(double* h_energy, double* h_aratio) override {
+    const int V = dm.V, R = dm.R;
+    const long long VP = (long long)V * g.P, VH = (long long)V * g.H, RP = (long long)R * g.P, RH = (long long)R * g.H;
+    const C* ph_p = uhat[0] + g.nd * RH;
+    irfft(ph_p, R, mon_gp, M_DX);
+    irfft(ph_p, R, mon_gp + RP, M_DY);
+    irfft(hat4[0], V, mon_lap, M_LAP);
+    irfft(hat4[0], V, mon_lap + VP, M_LAP, 1.0, hat4[1], 2.0, -1.0);
+    bool s2 = ph.S2 != 0.0;
+    if (s2) {
+      irfft(hat4[0], V, mon_g4, M_DX);
+      irfft(hat4[0], V, mon_g4 + VP, M_DY);
+      irfft(hat4[0], V, mon_g4 + 2 * VP, M_DX, 1.0, hat4[1], 2.0, -1.0);
+      irfft(hat4[0], V, mon_g4 + 3 * VP, M_DY, 1.0, hat4[1], 2.0, -1.0);
+    }
+    rfft(phys4[0], V, tmpH2);
+    irfft(tmpH2, V, mon_ga, M_DX);
+    irfft(tmpH2, V, mon_ga + VP, M_DY);
+    EW e = ew(g.P);
+    k_mon_v<T><<<dim3(e.bpf, V), 256, 0, st>>>(phys4[0], phys4[1], phys4[0] + VP, phys4[1] + VP, mon_lap, mon_lap + VP,
+                                               s2 ? mon_g4 : nullptr, mon_ga, VP, ph, e, part);
+    VSAV_LAUNCH_CHECK();
+    fin(9, V, e, fd);
+    k_mon_r<T><<<dim3(e.bpf, R), 256, 0, st>>>(uphys[0], uphys[1], mon_gp, g.nd, RP, e, part);
+    VSAV_LAUNCH_CHECK();
+    fin(3, R, e, fd2);
+    k_fin_mon<<<(R + 63) / 64, 64, 0, st>>>(fd, fd2, sc[0], sc[1], d_dt, d_A0, ph, rn, energy, aratio, area);
+    VSAV_LAUNCH_CHECK();
+    if (h_energy) VSAV_CUDA(cudaMemcpyAsync(h_energy, energy, R * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (h_aratio) VSAV_CUDA(cudaMemcpyAsync(h_aratio, aratio, R * sizeof(double), cudaMemcpyDeviceToHost, st));
+    VSAV_CUDA(cudaStreamSynchronize(st));
+  }
+
+  // simulation.jl:22-53
+  void init_state(int hats_given) override {
+    const int V = dm.V, R = dm.R;
+    const long long VP = (long long)V * g.P, VH = (long long)V * g.H;
+    if (!hats_given) {
+      rfft(phys4[0], V, hat4[0]);
+      rfft(phys4[0] + VP, V, hat4[0] + VH);
+      rfft(uphys[0], (long long)(g.nd + 1) * R, uhat[0]);
+    }
+    // A0 = calculate_area(phi)
+    EW e = ew(g.P);
+    rfft(phys4[0], V, tmpH2);
+    irfft(tmpH2, V, mon_ga, M_DX);
+    irfft(tmpH2, V, mon_ga + VP, M_DY);
+    k_surf<T><<<dim3(e.bpf, V), 256, 0, st>>>(phys4[0], mon_ga, mon_ga + VP, nullptr, nullptr, ph, e, part);
+    VSAV_LAUNCH_CHECK();
+    fin(3, V, e, fd);
+    k_area0<<<(V + 63) / 64, 64, 0, st>>>(fd, ph.cell, d_A0, V);
+    VSAV_LAUNCH_CHECK();
+    compute_H(phys4[0], nullptr, phys4[0] + VP, nullptr, false);
+    k_init_scalars<<<(R + 63) / 64, 64, 0, st>>>(scH, sc[0], R);
+    k_init_munu<T><<<gridfor(VH), 256, 0, st>>>(hat4[0], Hh, sc[0], ph, rn, g);
+    VSAV_LAUNCH_CHECK();
+    irfft(hat4[0] + 2 * VH, 2LL * V, phys4[0] + 2 * VP);
+    // old = deepcopy(present)
+    VSAV_CUDA(cudaMemcpyAsync(phys4[1], phys4[0], 4 * VP * sizeof(T), cudaMemcpyDeviceToDevice, st));
+    VSAV_CUDA(cudaMemcpyAsync(hat4[1], hat4[0], 4 * VH * sizeof(C), cudaMemcpyDeviceToDevice, st));
+    VSAV_CUDA(cudaMemcpyAsync(uphys[1], uphys[0], (g.nd + 1) * (long long)R * g.P * sizeof(T), cudaMemcpyDeviceToDevice, st));
+    VSAV_CUDA(cudaMemcpyAsync(uhat[1], uhat[0], (g.nd + 1) * (long long)R * g.H * sizeof(C), cudaMemcpyDeviceToDevice, st));
+    VSAV_CUDA(cudaMemcpyAsync(sc[1], sc[0], 4 * R * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    VSAV_CUDA(cudaStreamSynchronize(st));
+  }
+
+  // ------------------------------------------------------------------ psi BiCGSTAB (2D)
+  void matvec(const C* in, C* out, int mode, const C* svec) {
+    const int V = dm.V;
+    const long long F = 3LL * V, n = psi_n();
+    const bool full = psi_full();
+    C* t1 = vt12;
+    C* t2 = vt12 + F * n;
+    int geo = full ? 3 : 0;
+    cols(true, geo, F, in, nullptr, 1, 0, full ? M_DX0 : M_DXZ, ph.S4, t1, 1);
+    cols(true, geo, F, in, nullptr, 1, 0, M_DY, ph.S4, t2, 1);
+    // fused x pass on t1|t2
+    {
+      int L = full ? g.Nx : g.Nx / 2, logL = ilog2(L);
+      long long nrows = 2 * F * g.Ny;
+      int nl = rows_nl(L, nrows, g.Ny);
+      int thr = std::max(32, nl * L / FFTCfg<T>::E);
+      long long grid = (nrows + nl - 1) / nl;
+      SysMap sm{V, dm.R, d_run_of};
+      int rowlen = full ? g.Nx : g.kp;
+      if (full)
+        k_rows_mul<T, true><<<(unsigned)grid, thr, rows_smem(L, nl), st>>>(t1, Mpsi, (T)0, (T)(1.0 / g.P), logL, nl, nrows,
+                                                                           rowlen, g.Ny, sm, bupd, tab);
+      else
+        k_rows_mul<T, false><<<(unsigned)grid, thr, rows_smem(L, nl), st>>>(t1, Mpsi, (T)0, (T)(1.0 / g.P), logL, nl, nrows,
+                                                                            rowlen, g.Ny, sm, bupd, tab);
+      VSAV_LAUNCH_CHECK();
+    }
+    cols(false, geo, 2 * F, t1, nullptr, 1, 0, M_ONE, 1, t1, 1);
+    EW e = ew(n);
+    VGeom vg{full ? 1 : 0, g.Nx, g.Ny, g.kp, g.nkx, n, g.kxs, g.kys};
+    SysMap sm{V, dm.R, d_run_of};
+    const double* pre = (opt.psi_precond >= 0) ? mmax_r : nullptr;
+    k_psi_combine<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(in, t1, t2, out, vb, svec, mode, d_adt, pre, ph.S4, vg, sm,
+                                                                bupd, e, part);
+    VSAV_LAUNCH_CHECK();
+  }
+
+  void psi_solve() {
+    const int V = dm.V, R = dm.R, S = 3 * R;
+    const long long F = 3LL * V, VH = (long long)V * g.H, n = psi_n();
+    const bool full = psi_full();
+    // b = fft(irfft(rhs)) (FULL) / rfft(irfft(rhs)) (HALF)   (Solvers.jl:70-71)
+    irfft(rhs, F, tmpP);
+    if (full) {
+      rows_c2c<false>(nullptr, tmpP, vb, 1.0, F * g.Ny);
+      cols(false, 3, F, vb, nullptr, 1, 0, M_ONE, 1, vb, 1);
+    } else {
+      rfft(tmpP, F, vb);
+    }
+    C* x = full ? vx : cache + 5 * VH;
+    EW e = ew(n);
+    VGeom vg{full ? 1 : 0, g.Nx, g.Ny, g.kp, g.nkx, n, g.kxs, g.kys};
+    SysMap sm{V, R, d_run_of};
+    k_psi_init<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(vb, x, vr, vp, d_adt, mmax_r, ph.S4, vg, sm, e, part);
+    VSAV_LAUNCH_CHECK();
+    fin(4, (int)F, e, fd);
+    k_bi_init<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, bupd, sm, S, (int)F, opt.psi_atol, opt.psi_rtol, opt.psi_itmax);
+    VSAV_LAUNCH_CHECK();
+    for (int it = 0; it < opt.psi_itmax; ++it) {
+      matvec(vp, vv, 0, nullptr);                       // v = M^-1 A p ; <c, v>
+      fin(4, (int)F, e, fd);
+      k_bi_alpha<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, sm, S, (int)F);
+      k_psi_s<T><<<gridfor(F * n), 256, 0, st>>>(vr, vv, vs, bst, sm, n, (int)F);
+      VSAV_LAUNCH_CHECK();
+      matvec(vs, vt, 1, vs);                            // t = M^-1 A s ; <t,s>, <t,t>
+      fin(4, (int)F, e, fd);
+      k_bi_omega<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, sm, S, (int)F);
+      k_psi_update<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(x, vr, vp, vs, vt, vb, bst, vg, sm, e, part);
+      VSAV_LAUNCH_CHECK();
+      fin(4, (int)F, e, fd);
+      VSAV_CUDA(cudaMemsetAsync(d_any, 0, sizeof(int), st));
+      k_bi_beta<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, bupd, sm, S, (int)F, opt.psi_itmax, d_any);
+      k_psi_p<T><<<gridfor(F * n), 256, 0, st>>>(vp, vr, vv, bst, bupd, sm, n, (int)F);
+      VSAV_LAUNCH_CHECK();
+      if (opt.check_every_iter) {
+        VSAV_CUDA(cudaMemcpyAsync(h_pinned_any, d_any, sizeof(int), cudaMemcpyDeviceToHost, st));
+        VSAV_CUDA(cudaStreamSynchronize(st));
+        if (!*h_pinned_any) break;
+      }
+      // refresh the activity flags for the operator kernels of the next iteration
+      k_bi_flags<<<(S + 63) / 64, 64, 0, st>>>(bst, bupd, S);
+    }
+    if (full) { k_trunc<T><<<gridfor(F * g.Ny * g.kp), 256, 0, st>>>(vx, cache + 5 * VH, g.Nx, g.Ny, g.kp, g.nkx, (int)F); VSAV_LAUNCH_CHECK(); }
+  }
+
+  // ------------------------------------------------------------------ host transfer
+  // host layouts (float64): V fields [V][Nz][Ny][Nx]; hats [V][Nz][Ny][nkx] complex;
+  // u [R][nd][...]; p [R][...]
+  void xfer(int level, int fid, void* host, int dir, int is_device = 0) {
+    const int V = dm.V, R = dm.R, nd = g.nd;
+    const long long VP = (long long)V * g.P, VH = (long long)V * g.H, RP = (long long)R * g.P, RH = (long long)R * g.H;
+    long long rows = (long long)g.Nz * g.Ny;
+    bool hat = (fid == F_PHI_HAT || fid == F_PSI_HAT || fid == F_U_HAT || fid == F_P_HAT || fid == F_MU_HAT || fid == F_NU_HAT);
+    int Fo, Fi; void* dst;
+    switch (fid) {
+      case F_PHI: case F_PHI_HAT: Fo = V; Fi = 1; dst = hat ? (void*)hat4[level] : (void*)phys4[level]; break;
+      case F_PSI: case F_PSI_HAT: Fo = V; Fi = 1; dst = hat ? (void*)(hat4[level] + VH) : (void*)(phys4[level] + VP); break;
+      case F_MU: case F_MU_HAT: Fo = V; Fi = 1; dst = hat ? (void*)(hat4[level] + 2 * VH) : (void*)(phys4[level] + 2 * VP); break;
+      case F_NU: case F_NU_HAT: Fo = V; Fi = 1; dst = hat ? (void*)(hat4[level] + 3 * VH) : (void*)(phys4[level] + 3 * VP); break;
+      case F_U: case F_U_HAT: Fo = R; Fi = nd; dst = hat ? (void*)uhat[level] : (void*)uphys[level]; break;
+      case F_P: case F_P_HAT: Fo = R; Fi = 1; dst = hat ? (void*)(uhat[level] + nd * RH) : (void*)(uphys[level] + nd * RP); break;
+      default: throw std::runtime_error("unknown field id");
+    }
+    size_t nbytes = hat ? (size_t)Fo * Fi * rows * g.nkx * 16 : (size_t)Fo * Fi * g.P * 8;
+    if (dir == 0) VSAV_CUDA(cudaMemcpyAsync(stage, host, nbytes, is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+    long long tot = hat ? (long long)Fo * Fi * rows * g.nkx : (long long)Fo * Fi * g.P;
+    if (hat) k_import_hat<T><<<gridfor(tot), 256, 0, st>>>(stage, (C*)dst, Fo, Fi, rows, g.nkx, g.kp, dir);
+    else k_import_real<T><<<gridfor(tot), 256, 0, st>>>(stage, (T*)dst, Fo, Fi, g.P, dir);
+    VSAV_LAUNCH_CHECK();
+    if (dir == 1) VSAV_CUDA(cudaMemcpyAsync(host, stage, nbytes, cudaMemcpyDeviceToHost, st));
+    VSAV_CUDA(cudaStreamSynchronize(st));
+  }
+  void set_field(int level, int fid, const void* host, int is_device) override { xfer(level, fid, (void*)host, 0, is_device); }
+  void get_field(int level, int fid, void* host) override { xfer(level, fid, host, 1); }
+  void set_scalars(int level, const double* q4) override {
+    VSAV_CUDA(cudaMemcpyAsync(sc[level], q4, 4 * dm.R * sizeof(double), cudaMemcpyHostToDevice, st));
+    VSAV_CUDA(cudaStreamSynchronize(st));
+  }
+  void get_scalars(int level, double* q4) override {
+    VSAV_CUDA(cudaMemcpyAsync(q4, sc[level], 4 * dm.R * sizeof(double), cudaMemcpyDeviceToHost, st));
+    VSAV_CUDA(cudaStreamSynchronize(st));
+  }
+  void set_dt(const double* dt) override {
+    VSAV_CUDA(cudaMemcpyAsync(d_dt, dt, dm.R * sizeof(double), cudaMemcpyHostToDevice, st));
+    VSAV_CUDA(cudaStreamSynchronize(st));
+  }
+  void get_dt(double* dt) override {
+    VSAV_CUDA(cudaMemcpyAsync(dt, d_dt, dm.R * sizeof(double), cudaMemcpyDeviceToHost, st));
+    VSAV_CUDA(cudaStreamSynchronize(st));
+  }
+  void set_A0(const double* a0) override {
+    VSAV_CUDA(cudaMemcpyAsync(d_A0, a0, dm.V * sizeof(double), cudaMemcpyHostToDevice, st));
+    VSAV_CUDA(cudaStreamSynchronize(st));
+  }
+  void get_A0(double* a0) override {
+    VSAV_CUDA(cudaMemcpyAsync(a0, d_A0, dm.V * sizeof(double), cudaMemcpyDeviceToHost, st));
+    VSAV_CUDA(cudaStreamSynchronize(st));
+  }
+
+  // intermediate results, for the step-level API and parity tests
+  //  what 0: Step1Cache field idx (0..15, cache order), 1: Step3 field idx (s3 order), 2: u_tilde hat (idx 0/1),
+  //       3: u_tilde physical (idx 0/1), 4: H fields physical (H1,H2,H3,G)
+  void get_work(int what, int idx, void* host) override {
+    const int V = dm.V, R = dm.R, nd = g.nd;
+    const long long VH = (long long)V * g.H, VP = (long long)V * g.P, RH = (long long)R * g.H, RP = (long long)R * g.P;
+    long long rows = (long long)g.Nz * g.Ny;
+    if (what == 0 || what == 1 || what == 2) {
+      const C* src = what == 0 ? cache + idx * VH : (what == 1 ? s3 + idx * VH : uth + idx * nd * RH);
+      int Fo = what == 2 ? R : V, Fi = what == 2 ? nd : 1;
+      k_import_hat<T><<<gridfor((long long)Fo * Fi * rows * g.nkx), 256, 0, st>>>(stage, (C*)src, Fo, Fi, rows, g.nkx, g.kp, 1);
+      VSAV_LAUNCH_CHECK();
+      VSAV_CUDA(cudaMemcpyAsync(host, stage, (size_t)Fo * Fi * rows * g.nkx * 16, cudaMemcpyDeviceToHost, st));
+    } else {
+      const T* src = what == 3 ? utp + idx * nd * RP : H4 + idx * VP;
+      int Fo = what == 3 ? R : V, Fi = what == 3 ? nd : 1;
+      k_import_real<T><<<gridfor((long long)Fo * Fi * g.P), 256, 0, st>>>(stage, (T*)src, Fo, Fi, g.P, 1);
+      VSAV_LAUNCH_CHECK();
+      VSAV_CUDA(cudaMemcpyAsync(host, stage, (size_t)Fo * Fi * g.P * 8, cudaMemcpyDeviceToHost, st));
+    }
+    VSAV_CUDA(cudaStreamSynchronize(st));
+  }
+  //  what 0: step-2 R values [R][6]; 1: Q [R]; 2: theta [R][2]; 3: A (last area) [V]; 4: M_max [R];
+  //       5: psi solver stats [3R][4] (iters, solved, status, rnorm/eps)
+  void get_scalar_work(int what, double* out) override {
+    const int R = dm.R, V = dm.V;
+    if (what == 5) {
+      std::vector<BiState> hb(3 * R);
+      VSAV_CUDA(cudaMemcpyAsync(hb.data(), bst, 3 * R * sizeof(BiState), cudaMemcpyDeviceToHost, st));
+      VSAV_CUDA(cudaStreamSynchronize(st));
+      for (int s = 0; s < 3 * R; ++s) {
+        out[4 * s] = hb[s].iters; out[4 * s + 1] = hb[s].solved; out[4 * s + 2] = hb[s].status;
+        out[4 * s + 3] = hb[s].rnorm / std::max(hb[s].eps, 1e-300);
+      }
+      return;
+    }
+    const double* src = what == 0 ? r2 : (what == 1 ? qv : (what == 2 ? theta : (what == 3 ? area : mmax_r)));
+    size_t n = what == 0 ? 6 * R : (what == 2 ? 2 * R : (what == 3 ? V : R));
+    VSAV_CUDA(cudaMemcpyAsync(out, src, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    VSAV_CUDA(cudaStreamSynchronize(st));
+  }
+
+  // standalone transforms on host/device double buffers (for parity tests of the FFT layer)
+  //  kind 0: rfft  [nf][Nz][Ny][Nx] -> [nf][Nz][Ny][nkx] complex
+  //  kind 1: irfft (inverse of the above, normalised)
+  //  kind 10+m: irfft of Mult m * input
+  void transform(int kind, int nf, const double* in, double* out) override {
+    const long long rows = (long long)g.Nz * g.Ny;
+    if ((long long)nf > 3LL * dm.V) throw std::runtime_error("transform batch too large");
+    T* rbuf = tmpP;
+    C* hbuf = rhs;
+    if (kind == 0) {
+      VSAV_CUDA(cudaMemcpyAsync(stage, in, (size_t)nf * g.P * 8, cudaMemcpyDefault, st));
+      k_import_real<T><<<gridfor(nf * g.P), 256, 0, st>>>(stage, rbuf, nf, 1, g.P, 0);
+      rfft(rbuf, nf, hbuf);
+      k_import_hat<T><<<gridfor(nf * rows * g.nkx), 256, 0, st>>>(stage, hbuf, nf, 1, rows, g.nkx, g.kp, 1);
+      VSAV_CUDA(cudaMemcpyAsync(out, stage, (size_t)nf * rows * g.nkx * 16, cudaMemcpyDefault, st));
+    } else {
+      int mult = kind == 1 ? M_ONE : kind - 10;
+      VSAV_CUDA(cudaMemcpyAsync(stage, in, (size_t)nf * rows * g.nkx * 16, cudaMemcpyDefault, st));
+      VSAV_CUDA(cudaMemsetAsync(hbuf, 0, (size_t)nf * g.H * sizeof(C), st));
+      k_import_hat<T><<<gridfor(nf * rows * g.nkx), 256, 0, st>>>(stage, hbuf, nf, 1, rows, g.nkx, g.kp, 0);
+      irfft(hbuf, nf, rbuf, mult);
+      k_import_real<T><<<gridfor(nf * g.P), 256, 0, st>>>(stage, rbuf, nf, 1, g.P, 1);
+      VSAV_CUDA(cudaMemcpyAsync(out, stage, (size_t)nf * g.P * 8, cudaMemcpyDefault, st));
+    }
+    VSAV_LAUNCH_CHECK();
+    VSAV_CUDA(cudaStreamSynchronize(st));
+  }
+
+  StepStatus status() override {
+    StepStatus s;
+    int e = 0;
+    VSAV_CUDA(cudaMemcpyAsync(&e, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    VSAV_CUDA(cudaStreamSynchronize(st));
+    s.err_flags = e;
+    if (g.nd == 2) {
+      int S = 3 * dm.R;
+      std::vector<BiState> hb(S);
+      VSAV_CUDA(cudaMemcpyAsync(hb.data(), bst, S * sizeof(BiState), cudaMemcpyDeviceToHost, st));
+      VSAV_CUDA(cudaStreamSynchronize(st));
+      s.psi_systems = S;
+      for (auto& b : hb) {
+        s.psi_max_iters = std::max(s.psi_max_iters, b.iters);
+        if (!b.solved) s.psi_not_converged++;
+      }
+    }
+    return s;
+  }
+  void sync() override { VSAV_CUDA(cudaStreamSynchronize(st)); }
+};
+
+}  // namespace vsav

@@ -1,0 +1,237 @@
+"""GPU parity of libvsav against the CPU oracle and its golden fixtures,
+through the C ABI.  Bars: FP64 path within 1e-10 relative L2 of the oracle on
+every field and SAV scalar (the reference-faithful path); FP32 bulk path
+within 1e-5; transforms at round-off (2.5e-16 FP64, 1.2e-7 FP32 measured)."""
+import math
+import warnings
+
+import numpy as np
+import pytest
+
+from helpers import Cfg, load_golden, rel
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("phi", "psi", "mu", "nu", "u", "p")
+
+
+def make(kw, **opt):
+    from vsav import Handle
+    return Handle(Cfg(**kw), **opt)
+
+
+def kat_cfg(Nx=128, Ny=64):
+    # the shared fixture of test/test_Types_Ops.jl:28-41 (non-square, L = 2 pi)
+    return dict(N=1, epsilon=0.05, M_phi=1.0, M0_psi=1.0, eta=1.0, gamma_surf=1.0, gamma_area=1.0,
+                gamma_bend=1.0, gamma_in=1.0, beta_in=0.0, psi_in_v=[0.1], gamma_out=1.0, beta_out=0.0,
+                psi_out_v=[0.8], lamda=1.0, S1=1.0, S2=1.0, S3=1.0, S4=1.0, C1=1.0, C2=1.0, C3=1.0,
+                dt=1e-3, T=1.0, Nx=Nx, Ny=Ny, Lx=2 * math.pi, Ly=2 * math.pi, tol=1e-10, goal="s")
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 2e-15), ("fp32", 6e-7)])
+def test_transform_parity_2d(prec, tol):
+    from oracle import vsav_oracle as O
+    kw = kat_cfg()
+    h = make(kw, precision=prec)
+    ops = O.build_operators(O.Config(**kw))
+    rng = np.random.default_rng(0)
+    f = rng.standard_normal((3, 64, 128))
+    assert rel(h.rfft(f), np.fft.rfft2(f)) < tol
+    H = rng.standard_normal((3, 64, 65)) + 1j * rng.standard_normal((3, 64, 65))   # non-Hermitian
+    assert rel(h.irfft(H), np.fft.irfft2(H, s=(64, 128))) < tol
+    for m, mul in (("dx", ops.D1[0]), ("dy", ops.D1[1]), ("lap", ops.Laplacian), ("bih", ops.Biharmonic)):
+        assert rel(h.irfft(H, m), np.fft.irfft2(mul * H, s=(64, 128))) < tol, m
+    h.close()
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 2e-15), ("fp32", 6e-7)])
+def test_transform_parity_3d(prec, tol):
+    kw, g = load_golden("single3d_n32")
+    h = make(kw, precision=prec)
+    rng = np.random.default_rng(1)
+    f = rng.standard_normal((1, 32, 32, 32))
+    assert rel(h.rfft(f), np.fft.rfftn(f, axes=(1, 2, 3))) < tol
+    H = rng.standard_normal((1, 32, 32, 17)) + 1j * rng.standard_normal((1, 32, 32, 17))
+    assert rel(h.irfft(H), np.fft.irfftn(H, s=(32, 32, 32), axes=(1, 2, 3))) < tol
+    h.close()
+
+
+def test_spectral_derivative_kats_gpu():
+    """test_Types_Ops.jl G4/G5 on the device FP64 transforms, same bounds."""
+    from test_oracle_kat import kat_fields
+    from oracle import vsav_oracle as O
+    kw = kat_cfg()
+    cfg = O.Config(**kw)
+    h = make(kw)
+    rng = np.random.default_rng(1)
+    u = rng.standard_normal((1, 64, 128))
+    assert np.max(np.abs(h.irfft(h.rfft(u)) - u)) < 1e-13
+    c = np.full((1, 64, 128), 3.7)
+    assert np.max(np.abs(h.irfft(h.rfft(c)) - c)) < 1e-15
+    k = kat_fields(cfg)
+    fh = h.rfft(k["f"])
+    assert abs(np.sort(np.abs(fh).ravel())[::-1][0] - 1.0) < 1e-10
+    assert np.max(np.abs(h.irfft(fh, "dx") - k["dx"])) < 1e-15
+    assert np.max(np.abs(h.irfft(fh, "dy") - k["dy"])) < 1e-15
+    assert np.max(np.abs(h.irfft(fh, "lap") - k["lap"])) < 1e-14
+    assert np.max(np.abs(h.irfft(fh, "bih") - k["bih"])) < 1e-11
+    h.close()
+
+
+@pytest.mark.parametrize("name", ["single2d_n64", "multi2d_n64_N2", "single3d_n32"])
+def test_fp64_step_parity_vs_golden(name):
+    kw, g = load_golden(name)
+    steps = int(g["steps"])
+    h = make(kw, precision="fp64")
+    h.init_state(g["phi0"], g["psi0"])
+    np.testing.assert_allclose(h.get_A0(), g["A0"], rtol=1e-12)
+    E, A = h.run(1, steps, monitor=True)
+    for k in FIELDS:
+        assert rel(h.get_field(k), g[k]) < 1e-10, (k, rel(h.get_field(k), g[k]))
+    np.testing.assert_allclose(h.get_scalars()[0], g["scalars"], rtol=1e-10)
+    np.testing.assert_allclose(E[:, 0], g["energy"], rtol=1e-10)
+    np.testing.assert_allclose(A[:, 0], g["area"], rtol=1e-8, atol=1e-13)
+    if "3d" not in name:
+        # same BiCGSTAB iteration counts as the oracle in the last step
+        assert list(h.psi_stats()[:, 0].astype(int)) == list(g["psi_iters"][-3:])
+    h.close()
+
+
+def test_fp64_step_intermediates():
+    """Every solve_stepK output of the first two steps (BDF1 then BDF2)."""
+    from oracle import vsav_oracle as O
+    from vsav import Handle
+    kw, g = load_golden("single2d_n64")
+    cfg = O.Config(**kw)
+    h = make(kw)
+    h.init_state(g["phi0"], g["psi0"])
+    orc = O.Oracle(cfg)
+    pres = O.make_state(cfg, g["phi0"], g["psi0"], orc.ops)
+    O.init_state(cfg, pres, orc.ops)
+    old = pres.copy()
+    for n in (1, 2):
+        pres.dt = cfg.dt
+        bdf = O.bdf_coeff(n)
+        c1 = orc.solve_step1(pres, old, bdf)
+        h.step1(n)
+        for k in Handle.CACHE:
+            assert rel(h.get_cache(k), c1[k]) < 1e-10, k
+        s2 = orc.solve_step2(pres, old, c1, bdf)
+        h.step2(n)
+        np.testing.assert_allclose(h.scalar_work(0), [s2[k] for k in ("R_11_np1", "R_21_np1", "R_31_np1",
+                                                                   "R_12_np1", "R_22_np1", "R_32_np1")], rtol=1e-10)
+        s3 = orc.solve_step3(c1, s2)
+        h.step3()
+        for k in Handle.STEP3:
+            assert rel(h.get_step3(k), s3[k]) < 1e-10, k
+        s4 = orc.solve_step4(pres, old, bdf)
+        h.step4(n)
+        assert rel(h.get_u_tilde(0, hat=True)[0], s4["u_tilde_1_hat"]) < 1e-10
+        assert rel(h.get_u_tilde(1, hat=True)[0], s4["u_tilde_2_hat"]) < 1e-10
+        Q = orc.solve_step5(pres, old, s3, s4, bdf)
+        h.step5(n)
+        assert abs(h.scalar_work(1)[0] - Q) <= 1e-10 * abs(Q)
+        s6 = orc.solve_step6(s2, s3, s4, Q)
+        h.step6()
+        s7 = orc.solve_step7(pres, s6, bdf)
+        h.step7(n)
+        O.update_state(old, pres)
+        for k in ("phi_hat", "psi_hat", "mu_hat", "nu_hat"):
+            setattr(pres, k, s6[k])
+        pres.u_hat, pres.p_hat = s7["u_hat"], s7["p_hat"]
+        for k in FIELDS:
+            setattr(pres, k, orc.ops.irfft(getattr(pres, k + "_hat")))
+        pres.R1, pres.R2, pres.R3, pres.Q = s6["R1"], s6["R2"], s6["R3"], Q
+        h.update_state()
+        for k in FIELDS + ("phi_hat", "u_hat", "p_hat"):
+            assert rel(h.get_field(k), getattr(pres, k)) < 1e-10, k
+    h.close()
+
+
+def test_ensemble_runs_are_independent():
+    """R runs of different vesicle counts in one handle advance exactly like
+    separate handles (per-run SAV scalars, velocity and psi systems)."""
+    from vsav import ics
+    kwa, phia, psia, _ = ics.workload("multi2d_512x4", seed=1, n_override=64, N_override=1, eps_override=0.2)
+    kwb, phib, psib, _ = ics.workload("multi2d_512x4", seed=2, n_override=64, N_override=2, eps_override=0.2)
+    for kw in (kwa, kwb):
+        kw["dt"] = 1e-6
+    kwe = dict(kwa, N=1, psi_in_v=kwa["psi_in_v"] + kwb["psi_in_v"], psi_out_v=kwa["psi_out_v"] + kwb["psi_out_v"])
+    he = make(kwe, run_sizes=[1, 2])
+    he.init_state(np.concatenate([phia, phib]), np.concatenate([psia, psib]))
+    Ee, _ = he.run(1, 3, monitor=True)
+    for r, (kw, phi, psi, sl) in enumerate(((kwa, phia, psia, slice(0, 1)), (kwb, phib, psib, slice(1, 3)))):
+        h = make(kw)
+        h.init_state(phi, psi)
+        E, _ = h.run(1, 3, monitor=True)
+        assert rel(he.get_field("phi")[sl], h.get_field("phi")) < 1e-12
+        assert rel(he.get_field("u")[r], h.get_field("u")[0]) < 1e-12
+        np.testing.assert_allclose(he.get_scalars()[r], h.get_scalars()[0], rtol=1e-12)
+        np.testing.assert_allclose(Ee[:, r], E[:, 0], rtol=1e-12)
+        h.close()
+    he.close()
+
+
+@pytest.mark.parametrize("name", ["single2d_n64", "multi2d_n64_N2", "single3d_n32"])
+def test_fp32_bulk_within_1e5_of_fp64_oracle(name):
+    """FP32 fields and FFTs, FP64 SAV inner products / 3x3 / Q: every field,
+    the SAV scalars and the modified energy within 1e-5 relative L2."""
+    kw, g = load_golden(name)
+    steps = int(g["steps"])
+    h = make(kw, precision="fp32", psi_rtol=1e-8, psi_itmax=60)
+    h.init_state(g["phi0"], g["psi0"])
+    E, A = h.run(1, steps, monitor=True)
+    for k in FIELDS:
+        err = rel(h.get_field(k), g[k])
+        assert err < 1e-5, (k, err)
+    np.testing.assert_allclose(h.get_scalars()[0], g["scalars"], rtol=1e-5)
+    np.testing.assert_allclose(E[:, 0], g["energy"], rtol=1e-5)
+    assert np.all(np.diff(E[:, 0]) <= 0)
+    h.close()
+
+
+def test_energy_non_increasing_fp64_128():
+    from vsav import ics
+    kw, phi, psi, _ = ics.workload("single2d_128")
+    kw["dt"] = 1e-6
+    h = make(kw)
+    h.init_state(phi, psi)
+    E, A = h.run(1, 20, monitor=True)
+    assert np.all(np.diff(E[:, 0]) <= 0)
+    h.close()
+
+
+def test_wc_negative_is_an_error():
+    from vsav import WCNegativeError
+    kw, g = load_golden("single2d_n64")
+    h = make(dict(kw, C3=-1e9))
+    with pytest.raises(WCNegativeError):
+        h.init_state(g["phi0"], g["psi0"])
+    h.close()
+
+
+def test_not_converged_is_a_warning():
+    """itmax reached: the reference warns and keeps the iterate (Solvers.jl:76)."""
+    from vsav import NotConvergedWarning
+    kw, g = load_golden("single2d_n64")
+    h = make(kw, psi_itmax=2)
+    h.init_state(g["phi0"], g["psi0"])
+    with pytest.warns(NotConvergedWarning):
+        h.step1(1)
+    st = h.psi_stats()
+    assert st[0, 0] == 2 and st[0, 1] == 0
+    h.close()
+
+
+def test_half_form_converges():
+    """The half-spectrum psi form converges in as many iterations as the
+    reference form on a resolved interface."""
+    from vsav import ics
+    kw, phi, psi, _ = ics.workload("multi2d_512x4", seed=0, n_override=128, N_override=2, eps_override=0.2)
+    kw["dt"] = 1e-6
+    h = make(kw, psi_form="half")
+    h.init_state(phi, psi)
+    h.step1(1)
+    st = h.psi_stats()
+    assert np.all(st[:, 1] == 1) and np.max(st[:, 0]) <= 12
+    h.close()
