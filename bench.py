@@ -1,0 +1,364 @@
+#!/usr/bin/env python
+"""Benchmark of the pseudo-spectral SAV vesicle time step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (N=1): 2D, 1024^2 grid, 8 vesicles (seeded non-overlapping ellipses,
+radii U[0.4,0.7]), dt = 1e-6, one time step = Steps 1-7 of the reference
+(src/Solvers.jl) + state update + the per-step monitoring of
+src/simulation.jl:146-148 (modified energy, area ratio).  Our arm runs the FP32
+bulk path (FP64 SAV inner products, 3x3 and Q solves) with the psi BiCGSTAB in
+the reference's full-spectrum form; the same workload on the FP64 path is
+timed beside it (the "plain FP64 diagonal BiCGSTAB GPU solver").
+
+N>1 (torchrun): replicas only -- each rank advances its own seeded run, no
+data-path collective; value = all ranks' steps / max-over-ranks device time.
+
+--impl reference: the CPU restatement of the reference (the oracle, NumPy
+FP64 on multi-threaded pocketfft) on the host cores, rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "julia-vesicles-growth-and-shrinkage_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "steps/s at 1024²×8 vesicles, learned vs diagonal precond, same GPU, ≤1e-5 err"
+WORKLOAD = "multi2d_1024x8"
+DT = 1e-6
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Cfg:
+    def __init__(self, **kw):
+        self.__dict__.update(kw)
+        self.Nz = kw.get("Nz", 0)
+        self.Lz = kw.get("Lz", 0.0)
+
+
+def workload(seed):
+    from vsav import ics
+    kw, phi, psi, _ = ics.workload(WORKLOAD, seed=seed)
+    kw["dt"] = DT
+    return kw, phi, psi
+
+
+# --------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{gpu_index}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------------- dist
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return ws, rank, local
+
+
+def max_over_ranks(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# --------------------------------------------------------------------- CPU
+def cpu_reference(steps, warmup, rank_seed=0):
+    """The oracle (NumPy FP64, scipy pocketfft with all host threads) on a
+    bounded sample of the workload: one of the 8 vesicle fields of the
+    1024^2 run per step (cost is linear in the vesicle count); the rate is
+    scaled to the 8-vesicle workload."""
+    from oracle import vsav_oracle as O
+    kw, phi, psi = workload(rank_seed)
+    N = kw["N"]
+    kw1 = dict(kw, N=1, psi_in_v=kw["psi_in_v"][:1], psi_out_v=kw["psi_out_v"][:1])
+    cfg = O.Config(**kw1)
+    cores = os.cpu_count() or 1
+    orc = O.Oracle(cfg, workers=cores)
+    pres = O.make_state(cfg, phi[:1], psi[:1], orc.ops)
+    O.init_state(cfg, pres, orc.ops)
+    old = pres.copy()
+    n = 1
+    for _ in range(warmup):
+        orc.step(pres, old, n, DT)
+        orc.monitor(pres, old)
+        n += 1
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        orc.step(pres, old, n, DT)
+        orc.monitor(pres, old)
+        n += 1
+    dt = time.perf_counter() - t0
+    sps = steps / dt / N
+    iters = orc.counter.psi_iters
+    return dict(value=sps, unit="steps/s", cores=cores, kind="port",
+                sample=f"1 of {N} vesicle fields at 1024^2, {steps} steps after {warmup} warm-up, "
+                       f"rate scaled by 1/{N}; FP64 NumPy/pocketfft with {cores} threads",
+                sec_per_sample_step=dt / steps, mean_psi_iters=float(np.mean(iters)) if iters else None)
+
+
+def run_reference(args):
+    ws, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    cb = cpu_reference(args.steps, args.warmup)
+    out = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "steps/s", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / cb["value"],
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": WORKLOAD, "grid": [1024, 1024], "vesicles": 8, "dt": DT,
+                      "impl": "CPU restatement of the reference (Julia absent); one vesicle field per sampled step"},
+           "cpu_baseline": cb,
+           "e2e": {"value": cb["value"], "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+# --------------------------------------------------------------------- ours
+def run_ours(args):
+    ws, rank, local = dist_init()
+    from vsav import Handle, _lib
+    hbm, peak_kind = peaks()
+    kw, phi, psi = workload(rank)
+    V = kw["N"]
+    h = Handle(Cfg(**kw), precision="fp32", psi_form="full", psi_rtol=1e-8, psi_itmax=60, device=local)
+    h.init_state(phi, psi)
+    n = 1
+    h.run(n, args.warmup, monitor=True)
+    n += args.warmup
+    clk = ClockSampler(local)
+    barrier(ws)
+    clk.start()
+    l0 = _lib.load().vsav_launch_count()
+    ms = h.time_run(n, args.steps, monitor=True)
+    launches = _lib.load().vsav_launch_count() - l0
+    n += args.steps
+    clocks = clk.stop()
+    barrier(ws)
+    ms_max = max_over_ranks(ms, ws)
+    value = ws * args.steps / (ms_max / 1000.0)
+    iters = h.psi_stats()[:, 0].tolist()
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
+                              "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "quick": True,
+                              "gpu_launches": int(launches), "clocks": clocks, "psi_iters_last_step": iters}), flush=True)
+        h.close()
+        return
+
+    # end to end through the public API, host buffers: per step dt in (pinned
+    # host memory), energy + area ratio out, as run_simulation's loop does
+    import ctypes as ct
+    try:
+        import torch
+        dt_host = torch.full((h.R,), DT, dtype=torch.float64).pin_memory()
+        dt_ptr = ct.cast(dt_host.data_ptr(), ct.POINTER(ct.c_double))
+        out_host = torch.zeros(2 * h.R, dtype=torch.float64).pin_memory()
+        e_ptr = ct.cast(out_host.data_ptr(), ct.POINTER(ct.c_double))
+        a_ptr = ct.cast(out_host.data_ptr() + 8 * h.R, ct.POINTER(ct.c_double))
+        pinned = True
+    except Exception:
+        dt_np = np.full(h.R, DT)
+        out_np = np.zeros(2 * h.R)
+        dt_ptr = dt_np.ctypes.data_as(ct.POINTER(ct.c_double))
+        e_ptr = out_np.ctypes.data_as(ct.POINTER(ct.c_double))
+        a_ptr = ct.cast(out_np.ctypes.data + 8 * h.R, ct.POINTER(ct.c_double))
+        pinned = False
+    lib = _lib.load()
+    st = _lib.VsavStatus()
+    barrier(ws)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        rc = lib.vsav_run(h.h, n, 1, dt_ptr, e_ptr, a_ptr, ct.byref(st))
+        if rc < 0:
+            raise RuntimeError(lib.vsav_last_error(h.h).decode())
+        n += 1
+    e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks(e2e_s, ws)
+    e2e = {"value": ws * args.steps / e2e_s, "unit": "steps/s", "h2d_bytes_per_step": 8 * h.R,
+           "d2h_bytes_per_step": 16 * h.R,
+           "api": "vsav_run(h, n, 1, dt, energy, area_ratio) per step (the run_simulation loop body), "
+                  + ("pinned" if pinned else "pageable") + " host buffers"}
+
+    # per-kernel-class device time over the same K steps (CUDA events per launch)
+    h.profile("reset")
+    h.profile(True)
+    h.run(n, args.steps, monitor=True)
+    n += args.steps
+    h.profile(False)
+    prof = h.profile_read()
+    h.profile("reset")
+    dom = max(prof, key=lambda k: prof[k]["ms"])
+    d = prof[dom]
+    per_launch_bytes = d["bytes"] / max(d["launches"], 1)
+    per_launch_ms = d["ms"] / max(d["launches"], 1)
+    achieved = per_launch_bytes / (per_launch_ms / 1000.0) / 1e9 if per_launch_ms > 0 else 0.0
+    traffic = None
+    tr_path = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tr_path):
+        try:
+            traffic = json.load(open(tr_path)).get(dom)
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": traffic,
+                "algorithmic_bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms,
+                "launches_per_step": d["launches"] / args.steps,
+                "share_of_profiled_time": d["ms"] / max(sum(p["ms"] for p in prof.values()), 1e-9),
+                "classes": prof}
+    fp32_state = {k: h.get_field(k) for k in ("phi", "psi", "u")}
+    h.close()
+
+    # FP64 reference-form path on the same workload (the plain FP64 diagonal BiCGSTAB GPU solver)
+    k64 = max(1, min(args.steps, 3))
+    h64 = Handle(Cfg(**kw), precision="fp64", psi_form="full", device=local)
+    h64.init_state(phi, psi)
+    h64.run(1, args.warmup, monitor=True)
+    ms64 = h64.time_run(1 + args.warmup, k64, monitor=True)
+    it64 = h64.psi_stats()[:, 0].tolist()
+    h64.close()
+    ms64 = max_over_ranks(ms64, ws)
+    fp64_sps = ws * k64 / (ms64 / 1000.0)
+
+    # accuracy of the FP32 path against the FP64 GPU path, same steps
+    acc_steps = 3
+    ha = Handle(Cfg(**kw), precision="fp32", psi_form="full", psi_rtol=1e-8, psi_itmax=60, device=local)
+    hb = Handle(Cfg(**kw), precision="fp64", psi_form="full", device=local)
+    for hh in (ha, hb):
+        hh.init_state(phi, psi)
+    Ea, _ = ha.run(1, acc_steps, monitor=True)
+    Eb, _ = hb.run(1, acc_steps, monitor=True)
+    acc = {}
+    for k in ("phi", "psi", "mu", "nu", "u", "p"):
+        a, b = ha.get_field(k), hb.get_field(k)
+        acc[k] = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+    sa, sb = ha.get_scalars()[0], hb.get_scalars()[0]
+    for i, k in enumerate(("Q", "R1", "R2", "R3")):
+        acc[k] = float(abs(sa[i] - sb[i]) / max(abs(sb[i]), 1e-300))
+    acc["energy"] = float(np.max(np.abs(Ea - Eb) / np.abs(Eb)))
+    acc["energy_non_increasing"] = bool(np.all(np.diff(Ea[:, 0]) <= 0))
+    ha.close()
+    hb.close()
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu = cpu_reference(steps=2, warmup=1)
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+               "config": {"workload": WORKLOAD, "grid": [1024, 1024], "vesicles": V, "runs_per_gpu": 1,
+                          "dt": DT, "precision": "FP32 fields/FFTs, FP64 SAV dots + 3x3 + Q",
+                          "psi_solver": "BiCGSTAB, reference full-spectrum form, diagonal spectral preconditioner, rtol 1e-8",
+                          "parallelism": f"replicas x{ws}",
+                          "l2": "inputs larger than L2 (device state ~3 GB per run)",
+                          "step": "Steps 1-7 + update + modified energy + area ratio"},
+               "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks, "roofline": roofline,
+               "cpu_baseline": cpu,
+               "psi_iters_last_step": iters,
+               "fp64_diag_gpu": {"value": fp64_sps, "unit": "steps/s", "steps": k64, "psi_iters_last_step": it64},
+               "speedup_vs_fp64_diag": value / fp64_sps,
+               "fp32_vs_fp64_rel_err": acc}
+        print(json.dumps(out), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--quick", action="store_true", help="main timed region only (for profiler runs)")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

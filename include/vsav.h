@@ -128,6 +128,18 @@ int vsav_update_state(vsav_handle* h);
  * step and writes [nsteps][R]. */
 int vsav_run(vsav_handle* h, int32_t n0, int32_t nsteps, const double* dt, double* energy,
              double* area_ratio, vsav_status* st);
+/* vsav_run bracketed by CUDA events on the handle's stream: device time in ms */
+int vsav_time_run(vsav_handle* h, int32_t n0, int32_t nsteps, const double* dt, int32_t monitor,
+                  double* device_ms);
+/* per-kernel-class timing (CUDA events around each launch of the class, plus
+ * the algorithmic bytes of the launch: inputs read once, outputs written once).
+ * enable: 1 on, 0 off, 2 reset counters.  kclass: 0 FFT column pass, 1 x-pass
+ * r2c, 2 x-pass c2r, 3 x-pass c2c, 4 fused psi x-pass (inverse, x M_psi,
+ * forward), 5 psi operator combine.  out3 = (launches, total ms, total bytes). */
+int vsav_profile(vsav_handle* h, int32_t enable);
+/* kernels launched by this library so far (all handles) */
+int64_t vsav_launch_count(void);
+int vsav_profile_read(vsav_handle* h, int32_t kclass, double* out3);
 /* compute_modified_energy(present, old) and the area ratio (simulation.jl:146-147), per run */
 int vsav_monitor(vsav_handle* h, double* energy, double* area_ratio);
 

@@ -58,6 +58,9 @@ class SolverBase {
   virtual void transform(int kind, int nf, const double* in, double* out) = 0;
   virtual StepStatus status() = 0;
   virtual void sync() = 0;
+  virtual void profile(int enable) = 0;
+  virtual void profile_read(int cls, double* out3) = 0;
+  virtual cudaStream_t stream() = 0;
 };
 
 struct Dims {
@@ -115,6 +118,50 @@ __global__ void k_import_hat(const double* src, cplx<T>* dst, int Fo, int Fi, lo
     }
   }
 
+
+// ---------------------------------------------------------------------------
+// per-kernel-class timing: CUDA events around every launch of the class on the
+// handle's stream, plus the algorithmic bytes of each launch (inputs read once
+// + outputs written once).  Off unless enabled.
+// ---------------------------------------------------------------------------
+enum KClass : int { KC_COLS = 0, KC_ROWS_R2C, KC_ROWS_C2R, KC_ROWS_C2C, KC_ROWS_MUL, KC_PSI_VEC, KC_POINTWISE, KC_N };
+
+struct Prof {
+  bool on = false;
+  std::vector<cudaEvent_t> ev;
+  std::vector<std::pair<int, double>> rec;   // (class, bytes) per event pair
+  double ms[KC_N] = {0}, bytes[KC_N] = {0};
+  long long launches[KC_N] = {0};
+  void enable(bool e) {
+    on = e;
+    if (e && ev.empty()) {
+      ev.resize(2 * 16384);
+      for (auto& x : ev) VSAV_CUDA(cudaEventCreate(&x));
+    }
+  }
+  void begin(cudaStream_t st) {
+    if (!on) return;
+    if (2 * rec.size() + 2 > ev.size()) throw std::runtime_error("profiler event pool exhausted; collect more often");
+    VSAV_CUDA(cudaEventRecord(ev[2 * rec.size()], st));
+  }
+  void end(cudaStream_t st, int cls, double b) {
+    if (!on) return;
+    VSAV_CUDA(cudaEventRecord(ev[2 * rec.size() + 1], st));
+    rec.push_back({cls, b});
+  }
+  void collect() {
+    for (size_t i = 0; i < rec.size(); ++i) {
+      VSAV_CUDA(cudaEventSynchronize(ev[2 * i + 1]));
+      float t = 0;
+      VSAV_CUDA(cudaEventElapsedTime(&t, ev[2 * i], ev[2 * i + 1]));
+      ms[rec[i].first] += t; bytes[rec[i].first] += rec[i].second; launches[rec[i].first] += 1;
+    }
+    rec.clear();
+  }
+  void reset() { collect(); for (int k = 0; k < KC_N; ++k) { ms[k] = 0; bytes[k] = 0; launches[k] = 0; } }
+  ~Prof() { for (auto& x : ev) cudaEventDestroy(x); }
+};
+
 template <typename T>
 class Solver : public SolverBase {
  public:
@@ -148,6 +195,7 @@ class Solver : public SolverBase {
   double* stage = nullptr;   // host-format staging
   size_t stage_bytes = 0;
   double cur_a = 1, cur_b = -1, cur_c = 0;
+  Prof prof;
 
   template <typename X> X* dalloc(size_t n) {
     void* p = nullptr;
@@ -255,7 +303,7 @@ class Solver : public SolverBase {
   }
   int gridfor(long long n, int bs = 256) const { long long b = (n + bs - 1) / bs; return (int)std::min<long long>(b, 148 * 16); }
   void fin(int K, int F, const EW& e, double* out) {
-    k_fin_fields<<<F, 256, 0, st>>>(part, e.bpf, K, out);
+    k_fin_fields<<<F, 256, 0, st>>>(part, e.bpf, K, out); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
   }
 
@@ -272,16 +320,20 @@ class Solver : public SolverBase {
     int nl = rows_nl(L, nrows);
     int thr = std::max(32, nl * L / FFTCfg<T>::E);
     long long grid = (nrows + nl - 1) / nl;
-    k_rows_r2c<T><<<(unsigned)grid, thr, rows_smem(L, nl), st>>>(in0, in1, (T)a0, (T)a1, out, logL, nl, nrows, g.kp, tab);
+    prof.begin(st);
+    k_rows_r2c<T><<<(unsigned)grid, thr, rows_smem(L, nl), st>>>(in0, in1, (T)a0, (T)a1, out, logL, nl, nrows, g.kp, tab); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
+    prof.end(st, KC_ROWS_R2C, (double)nrows * (g.Nx * sizeof(T) * (in1 ? 2 : 1) + g.nkx * sizeof(C)));
   }
   void rows_c2r(const C* in, T* out, double scale, long long nrows) {
     int L = g.Nx / 2, logL = ilog2(L);
     int nl = rows_nl(L, nrows);
     int thr = std::max(32, nl * L / FFTCfg<T>::E);
     long long grid = (nrows + nl - 1) / nl;
-    k_rows_c2r<T><<<(unsigned)grid, thr, rows_smem(L, nl), st>>>(in, out, (T)scale, logL, nl, nrows, g.kp, tab);
+    prof.begin(st);
+    k_rows_c2r<T><<<(unsigned)grid, thr, rows_smem(L, nl), st>>>(in, out, (T)scale, logL, nl, nrows, g.kp, tab); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
+    prof.end(st, KC_ROWS_C2R, (double)nrows * (g.Nx * sizeof(T) + g.nkx * sizeof(C)));
   }
   template <bool INV>
   void rows_c2c(const C* in, const T* in_real, C* out, double scale, long long nrows) {
@@ -289,8 +341,10 @@ class Solver : public SolverBase {
     int nl = rows_nl(L, nrows);
     int thr = std::max(32, nl * L / FFTCfg<T>::E);
     long long grid = (nrows + nl - 1) / nl;
-    k_rows_c2c<T, INV><<<(unsigned)grid, thr, rows_smem(L, nl), st>>>(in, in_real, out, (T)scale, logL, nl, nrows, tab);
+    prof.begin(st);
+    k_rows_c2c<T, INV><<<(unsigned)grid, thr, rows_smem(L, nl), st>>>(in, in_real, out, (T)scale, logL, nl, nrows, tab); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
+    prof.end(st, KC_ROWS_C2C, (double)nrows * g.Nx * ((in_real ? sizeof(T) : sizeof(C)) + sizeof(C)));
   }
   // geo: 0 2D y (half), 1 3D z (half), 2 3D y (half), 3 2D y (full)
   ColArgs colargs(int geo, long long& nouter) const {
@@ -317,9 +371,13 @@ class Solver : public SolverBase {
     int thr = std::max(32, a.TW * L / FFTCfg<T>::E);
     size_t sm = (size_t)(a.TW * line_pitch(L)) * sizeof(C);
     long long grid = (long long)a.tiles * nouter;
-    if (inv) k_cols<T, true><<<(unsigned)grid, thr, sm, st>>>(in0, in1, (T)a0, (T)a1, mult, ms, out, (T)oscale, a, tab);
-    else k_cols<T, false><<<(unsigned)grid, thr, sm, st>>>(in0, in1, (T)a0, (T)a1, mult, ms, out, (T)oscale, a, tab);
+    long long valid_lines = (geo == 3) ? (long long)g.Nx : (long long)g.nkx * (geo == 1 ? g.Ny : 1);
+    double cb = (double)nouter * valid_lines * L * sizeof(C) * ((in1 ? 2 : 1) + 1);
+    prof.begin(st);
+    if (inv) { k_cols<T, true><<<(unsigned)grid, thr, sm, st>>>(in0, in1, (T)a0, (T)a1, mult, ms, out, (T)oscale, a, tab); VSAV_COUNT_LAUNCH(); }
+    else { k_cols<T, false><<<(unsigned)grid, thr, sm, st>>>(in0, in1, (T)a0, (T)a1, mult, ms, out, (T)oscale, a, tab); VSAV_COUNT_LAUNCH(); }
     VSAV_LAUNCH_CHECK();
+    prof.end(st, KC_COLS, cb);
   }
   // rfft over the nd spatial axes of nf real fields  (in = a0 in0 + a1 in1)
   void rfft(const T* in0, long long nf, C* out, const T* in1 = nullptr, double a0 = 1, double a1 = 0) {
@@ -349,29 +407,29 @@ class Solver : public SolverBase {
     dim3 gv(e.bpf, V);
     const T *phi = phi_in, *psi = psi_in;
     if (star) {
-      k_star<T><<<gv, 256, 0, st>>>(phi_in, phio, psi_in, psio, phis, psis, Mpsi, ph, rn, e, part);
+      k_star<T><<<gv, 256, 0, st>>>(phi_in, phio, psi_in, psio, phis, psis, Mpsi, ph, rn, e, part); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
       phi = phis; psi = psis;
     } else {
-      k_star<T><<<gv, 256, 0, st>>>(phi_in, nullptr, psi_in, nullptr, nullptr, nullptr, nullptr, ph, rn, e, part);
+      k_star<T><<<gv, 256, 0, st>>>(phi_in, nullptr, psi_in, nullptr, nullptr, nullptr, nullptr, ph, rn, e, part); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
     }
     fin(3, V, e, fd2);                                   // fd2[v*3+1..2] = f_osm, psi^2
-    if (star) { k_fin_max<<<V, 32, 0, st>>>(part, e.bpf, 3, 0, mmax_v); VSAV_LAUNCH_CHECK(); }
+    if (star) { k_fin_max<<<V, 32, 0, st>>>(part, e.bpf, 3, 0, mmax_v); VSAV_COUNT_LAUNCH(); VSAV_LAUNCH_CHECK(); }
     rfft(phi, V, tmpH2);
     irfft(tmpH2, V, d4, M_DX);
     irfft(tmpH2, V, d4 + VP, M_DY);
     irfft(tmpH2, V, d4 + 2 * VP, M_LAP);
     irfft(tmpH2, V, d4 + 3 * VP, M_BIH);
-    k_surf<T><<<gv, 256, 0, st>>>(phi, d4, d4 + VP, d4 + 2 * VP, omega, ph, e, part);
+    k_surf<T><<<gv, 256, 0, st>>>(phi, d4, d4 + VP, d4 + 2 * VP, omega, ph, e, part); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     fin(3, V, e, fd);                                    // fd[v*3+0..2] = surf, bend, E2
-    k_fin_H<<<(dm.R + 63) / 64, 64, 0, st>>>(fd, fd2, star ? mmax_v : nullptr, d_A0, ph, rn, scH, factor, area, d_err);
+    k_fin_H<<<(dm.R + 63) / 64, 64, 0, st>>>(fd, fd2, star ? mmax_v : nullptr, d_A0, ph, rn, scH, factor, area, d_err); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
-    if (star) { k_copy_mmax<<<(dm.R + 63) / 64, 64, 0, st>>>(scH, mmax_r, dm.R); VSAV_LAUNCH_CHECK(); }
+    if (star) { k_copy_mmax<<<(dm.R + 63) / 64, 64, 0, st>>>(scH, mmax_r, dm.R); VSAV_COUNT_LAUNCH(); VSAV_LAUNCH_CHECK(); }
     rfft(omega, V, tmpH2);
     irfft(tmpH2, V, lapomega, M_LAP);
-    k_H<T><<<gv, 256, 0, st>>>(phi, psi, omega, lapomega, d4 + 2 * VP, d4 + 3 * VP, scH, factor, H4, VP, ph, rn, e);
+    k_H<T><<<gv, 256, 0, st>>>(phi, psi, omega, lapomega, d4 + 2 * VP, d4 + 3 * VP, scH, factor, H4, VP, ph, rn, e); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     rfft(H4, 4LL * V, Hh);
   }
@@ -383,16 +441,16 @@ class Solver : public SolverBase {
     const int V = dm.V, R = dm.R, nd = g.nd;
     const long long VP = (long long)V * g.P, VH = (long long)V * g.H, RP = (long long)R * g.P;
     compute_H(phys4[0], phys4[1], phys4[0] + VP, phys4[1] + VP, true);
-    k_axpby<T><<<gridfor(nd * RP), 256, 0, st>>>(uphys[0], uphys[1], ustar, 2.0, -1.0, nd * RP);
+    k_axpby<T><<<gridfor(nd * RP), 256, 0, st>>>(uphys[0], uphys[1], ustar, 2.0, -1.0, nd * RP); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     // psi 12 flux: D1_d . rfft(M dG/dx_d)
     const C* Gh = Hh + 3 * VH;
     for (int d = 0; d < nd; ++d) irfft(Gh, V, gG + d * VP, M_DX + d);
     if (nd == 2) {
-      k_mul_field<T><<<gridfor(VP), 256, 0, st>>>(gG, Mpsi, 1.0, gG, VP, 1);
-      k_mul_field<T><<<gridfor(VP), 256, 0, st>>>(gG + VP, Mpsi, 1.0, gG + VP, VP, 1);
+      k_mul_field<T><<<gridfor(VP), 256, 0, st>>>(gG, Mpsi, 1.0, gG, VP, 1); VSAV_COUNT_LAUNCH();
+      k_mul_field<T><<<gridfor(VP), 256, 0, st>>>(gG + VP, Mpsi, 1.0, gG + VP, VP, 1); VSAV_COUNT_LAUNCH();
     } else {
-      k_mul_field<T><<<gridfor(3 * VP), 256, 0, st>>>(gG, nullptr, ph.M0_psi, gG, 3 * VP, 1);
+      k_mul_field<T><<<gridfor(3 * VP), 256, 0, st>>>(gG, nullptr, ph.M0_psi, gG, 3 * VP, 1); VSAV_COUNT_LAUNCH();
     }
     VSAV_LAUNCH_CHECK();
     rfft(gG, (long long)nd * V, flh);
@@ -400,16 +458,16 @@ class Solver : public SolverBase {
     for (int q = 0; q < 2; ++q)
       for (int d = 0; d < nd; ++d)
         irfft(hat4[0] + q * VH, V, gstar + (q * nd + d) * VP, M_DX + d, 1.0, hat4[1] + q * VH, 2.0, -1.0);
-    k_advect<T><<<gridfor(2 * VP), 256, 0, st>>>(gstar, ustar, adv, 2, nd, rn, g.P);
+    k_advect<T><<<gridfor(2 * VP), 256, 0, st>>>(gstar, ustar, adv, 2, nd, rn, g.P); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     rfft(adv, 2LL * V, advh);
-    k_set_adt<<<(R + 63) / 64, 64, 0, st>>>(d_dt, cur_a, d_adt, R);
+    k_set_adt<<<(R + 63) / 64, 64, 0, st>>>(d_dt, cur_a, d_adt, R); VSAV_COUNT_LAUNCH();
     k_step1_k<T><<<gridfor(VH), 256, 0, st>>>(hat4[0], hat4[1], Hh, flh, nd, advh, cache, rhs, d_dt, cur_a, cur_b, cur_c,
-                                              ph, rn, g);
+                                              ph, rn, g); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     if (nd == 2) {
       psi_solve();
-      k_nu<T><<<gridfor(VH), 256, 0, st>>>(cache, Gh, ph.S4, VH, g);
+      k_nu<T><<<gridfor(VH), 256, 0, st>>>(cache, Gh, ph.S4, VH, g); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
     }
   }
@@ -420,16 +478,16 @@ class Solver : public SolverBase {
     const long long VP = (long long)V * g.P;
     irfft(cache, 8LL * V, cphys);
     EW e = ew(g.P);
-    k_dot2<T><<<dim3(e.bpf, V), 256, 0, st>>>(H4, phys4[0], phys4[1], phys4[0] + VP, phys4[1] + VP, cphys, cur_b, cur_c, VP, e, part);
+    k_dot2<T><<<dim3(e.bpf, V), 256, 0, st>>>(H4, phys4[0], phys4[1], phys4[0] + VP, phys4[1] + VP, cphys, cur_b, cur_c, VP, e, part); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     fin(22, V, e, fd);
-    k_fin_step2<<<(dm.R + 63) / 64, 64, 0, st>>>(fd, sc[0], sc[1], cur_a, cur_b, cur_c, ph, rn, r2);
+    k_fin_step2<<<(dm.R + 63) / 64, 64, 0, st>>>(fd, sc[0], sc[1], cur_a, cur_b, cur_c, ph, rn, r2); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
   }
 
   void step3() override {
     const long long VH = (long long)dm.V * g.H;
-    k_step3<T><<<gridfor(VH), 256, 0, st>>>(cache, r2, s3, rn, g);
+    k_step3<T><<<gridfor(VH), 256, 0, st>>>(cache, r2, s3, rn, g); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
   }
 
@@ -444,10 +502,10 @@ class Solver : public SolverBase {
       irfft(hat4[0] + 2 * VH, V, gmu + d * VP, M_DX + d, 1.0, hat4[1] + 2 * VH, 2.0, -1.0);
       irfft(hat4[0] + 3 * VH, V, gnu + d * VP, M_DX + d, 1.0, hat4[1] + 3 * VH, 2.0, -1.0);
     }
-    k_conv_coupl<T><<<gridfor(RP), 256, 0, st>>>(ustar, gu, phis, psis, gmu, gnu, conv, coupl, rhs2, ph.lamda, nd, rn, g.P);
+    k_conv_coupl<T><<<gridfor(RP), 256, 0, st>>>(ustar, gu, phis, psis, gmu, gnu, conv, coupl, rhs2, ph.lamda, nd, rn, g.P); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     rfft(rhs2, (long long)nd * R, uth + nd * RH);
-    k_step4_k<T><<<gridfor(RH), 256, 0, st>>>(uhat[0], uhat[1], uth, d_dt, cur_a, cur_b, cur_c, ph, R, g);
+    k_step4_k<T><<<gridfor(RH), 256, 0, st>>>(uhat[0], uhat[1], uth, d_dt, cur_a, cur_b, cur_c, ph, R, g); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     irfft(uth, 2LL * nd * R, utp);
   }
@@ -458,27 +516,27 @@ class Solver : public SolverBase {
     const long long VP = (long long)V * g.P, VH = (long long)V * g.H, RP = (long long)R * g.P;
     irfft(s3 + 4 * VH, 4LL * V, mn);
     EW e = ew(g.P);
-    k_dot5v<T><<<dim3(e.bpf, V), 256, 0, st>>>(adv, mn, VP, e, part);
+    k_dot5v<T><<<dim3(e.bpf, V), 256, 0, st>>>(adv, mn, VP, e, part); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     fin(4, V, e, fd);
-    k_dot5r<T><<<dim3(e.bpf, R), 256, 0, st>>>(coupl, conv, utp, g.nd, RP, e, part);
+    k_dot5r<T><<<dim3(e.bpf, R), 256, 0, st>>>(coupl, conv, utp, g.nd, RP, e, part); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     fin(4, R, e, fd2);
-    k_fin_step5<<<(R + 63) / 64, 64, 0, st>>>(fd, fd2, sc[0], sc[1], d_dt, g.nd == 3, cur_a, cur_b, cur_c, ph, rn, qv, theta);
+    k_fin_step5<<<(R + 63) / 64, 64, 0, st>>>(fd, fd2, sc[0], sc[1], d_dt, g.nd == 3, cur_a, cur_b, cur_c, ph, rn, qv, theta); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
   }
 
   void step6() override {
     const long long VH = (long long)dm.V * g.H;
-    k_step6<T><<<gridfor(VH), 256, 0, st>>>(s3, qv, hat4[1], rn, g);
-    k_step6_scalars<<<(dm.R + 63) / 64, 64, 0, st>>>(r2, qv, sc[1], dm.R);
+    k_step6<T><<<gridfor(VH), 256, 0, st>>>(s3, qv, hat4[1], rn, g); VSAV_COUNT_LAUNCH();
+    k_step6_scalars<<<(dm.R + 63) / 64, 64, 0, st>>>(r2, qv, sc[1], dm.R); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
   }
 
   void step7(int n) override {
     set_bdf(n);
     const long long RH = (long long)dm.R * g.H;
-    k_step67<T><<<gridfor(RH), 256, 0, st>>>(uth, qv, uhat[0], uhat[1], d_dt, cur_a, ph, dm.R, g);
+    k_step67<T><<<gridfor(RH), 256, 0, st>>>(uth, qv, uhat[0], uhat[1], d_dt, cur_a, ph, dm.R, g); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
   }
 
@@ -511,13 +569,13 @@ class Solver : public SolverBase {
     irfft(tmpH2, V, mon_ga + VP, M_DY);
     EW e = ew(g.P);
     k_mon_v<T><<<dim3(e.bpf, V), 256, 0, st>>>(phys4[0], phys4[1], phys4[0] + VP, phys4[1] + VP, mon_lap, mon_lap + VP,
-                                               s2 ? mon_g4 : nullptr, mon_ga, VP, ph, e, part);
+                                               s2 ? mon_g4 : nullptr, mon_ga, VP, ph, e, part); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     fin(9, V, e, fd);
-    k_mon_r<T><<<dim3(e.bpf, R), 256, 0, st>>>(uphys[0], uphys[1], mon_gp, g.nd, RP, e, part);
+    k_mon_r<T><<<dim3(e.bpf, R), 256, 0, st>>>(uphys[0], uphys[1], mon_gp, g.nd, RP, e, part); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     fin(3, R, e, fd2);
-    k_fin_mon<<<(R + 63) / 64, 64, 0, st>>>(fd, fd2, sc[0], sc[1], d_dt, d_A0, ph, rn, energy, aratio, area);
+    k_fin_mon<<<(R + 63) / 64, 64, 0, st>>>(fd, fd2, sc[0], sc[1], d_dt, d_A0, ph, rn, energy, aratio, area); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     if (h_energy) VSAV_CUDA(cudaMemcpyAsync(h_energy, energy, R * sizeof(double), cudaMemcpyDeviceToHost, st));
     if (h_aratio) VSAV_CUDA(cudaMemcpyAsync(h_aratio, aratio, R * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -538,14 +596,14 @@ class Solver : public SolverBase {
     rfft(phys4[0], V, tmpH2);
     irfft(tmpH2, V, mon_ga, M_DX);
     irfft(tmpH2, V, mon_ga + VP, M_DY);
-    k_surf<T><<<dim3(e.bpf, V), 256, 0, st>>>(phys4[0], mon_ga, mon_ga + VP, nullptr, nullptr, ph, e, part);
+    k_surf<T><<<dim3(e.bpf, V), 256, 0, st>>>(phys4[0], mon_ga, mon_ga + VP, nullptr, nullptr, ph, e, part); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     fin(3, V, e, fd);
-    k_area0<<<(V + 63) / 64, 64, 0, st>>>(fd, ph.cell, d_A0, V);
+    k_area0<<<(V + 63) / 64, 64, 0, st>>>(fd, ph.cell, d_A0, V); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     compute_H(phys4[0], nullptr, phys4[0] + VP, nullptr, false);
-    k_init_scalars<<<(R + 63) / 64, 64, 0, st>>>(scH, sc[0], R);
-    k_init_munu<T><<<gridfor(VH), 256, 0, st>>>(hat4[0], Hh, sc[0], ph, rn, g);
+    k_init_scalars<<<(R + 63) / 64, 64, 0, st>>>(scH, sc[0], R); VSAV_COUNT_LAUNCH();
+    k_init_munu<T><<<gridfor(VH), 256, 0, st>>>(hat4[0], Hh, sc[0], ph, rn, g); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     irfft(hat4[0] + 2 * VH, 2LL * V, phys4[0] + 2 * VP);
     // old = deepcopy(present)
@@ -576,22 +634,28 @@ class Solver : public SolverBase {
       long long grid = (nrows + nl - 1) / nl;
       SysMap sm{V, dm.R, d_run_of};
       int rowlen = full ? g.Nx : g.kp;
-      if (full)
+      prof.begin(st);
+      if (full) {
         k_rows_mul<T, true><<<(unsigned)grid, thr, rows_smem(L, nl), st>>>(t1, Mpsi, (T)0, (T)(1.0 / g.P), logL, nl, nrows,
-                                                                           rowlen, g.Ny, sm, bupd, tab);
-      else
+                                                                           rowlen, g.Ny, sm, bupd, tab); VSAV_COUNT_LAUNCH();
+      } else {
         k_rows_mul<T, false><<<(unsigned)grid, thr, rows_smem(L, nl), st>>>(t1, Mpsi, (T)0, (T)(1.0 / g.P), logL, nl, nrows,
-                                                                            rowlen, g.Ny, sm, bupd, tab);
+                                                                            rowlen, g.Ny, sm, bupd, tab); VSAV_COUNT_LAUNCH();
+      }
       VSAV_LAUNCH_CHECK();
+      // reads+writes t1|t2 rows and reads M once per row (2F rows)
+      prof.end(st, KC_ROWS_MUL, (double)nrows * ((full ? g.Nx : g.nkx) * 2.0 * sizeof(C) + g.Nx * sizeof(T)));
     }
     cols(false, geo, 2 * F, t1, nullptr, 1, 0, M_ONE, 1, t1, 1);
     EW e = ew(n);
     VGeom vg{full ? 1 : 0, g.Nx, g.Ny, g.kp, g.nkx, n, g.kxs, g.kys};
     SysMap sm{V, dm.R, d_run_of};
     const double* pre = (opt.psi_precond >= 0) ? mmax_r : nullptr;
+    prof.begin(st);
     k_psi_combine<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(in, t1, t2, out, vb, svec, mode, d_adt, pre, ph.S4, vg, sm,
-                                                                bupd, e, part);
+                                                                bupd, e, part); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
+    prof.end(st, KC_PSI_VEC, (double)F * (full ? g.Pfull : (long long)g.Ny * g.nkx) * 5.0 * sizeof(C));
   }
 
   void psi_solve() {
@@ -610,26 +674,26 @@ class Solver : public SolverBase {
     EW e = ew(n);
     VGeom vg{full ? 1 : 0, g.Nx, g.Ny, g.kp, g.nkx, n, g.kxs, g.kys};
     SysMap sm{V, R, d_run_of};
-    k_psi_init<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(vb, x, vr, vp, d_adt, mmax_r, ph.S4, vg, sm, e, part);
+    k_psi_init<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(vb, x, vr, vp, d_adt, mmax_r, ph.S4, vg, sm, e, part); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     fin(4, (int)F, e, fd);
-    k_bi_init<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, bupd, sm, S, (int)F, opt.psi_atol, opt.psi_rtol, opt.psi_itmax);
+    k_bi_init<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, bupd, sm, S, (int)F, opt.psi_atol, opt.psi_rtol, opt.psi_itmax); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     for (int it = 0; it < opt.psi_itmax; ++it) {
       matvec(vp, vv, 0, nullptr);                       // v = M^-1 A p ; <c, v>
       fin(4, (int)F, e, fd);
-      k_bi_alpha<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, sm, S, (int)F);
-      k_psi_s<T><<<gridfor(F * n), 256, 0, st>>>(vr, vv, vs, bst, sm, n, (int)F);
+      k_bi_alpha<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, sm, S, (int)F); VSAV_COUNT_LAUNCH();
+      k_psi_s<T><<<gridfor(F * n), 256, 0, st>>>(vr, vv, vs, bst, sm, n, (int)F); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
       matvec(vs, vt, 1, vs);                            // t = M^-1 A s ; <t,s>, <t,t>
       fin(4, (int)F, e, fd);
-      k_bi_omega<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, sm, S, (int)F);
-      k_psi_update<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(x, vr, vp, vs, vt, vb, bst, vg, sm, e, part);
+      k_bi_omega<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, sm, S, (int)F); VSAV_COUNT_LAUNCH();
+      k_psi_update<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(x, vr, vp, vs, vt, vb, bst, vg, sm, e, part); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
       fin(4, (int)F, e, fd);
       VSAV_CUDA(cudaMemsetAsync(d_any, 0, sizeof(int), st));
-      k_bi_beta<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, bupd, sm, S, (int)F, opt.psi_itmax, d_any);
-      k_psi_p<T><<<gridfor(F * n), 256, 0, st>>>(vp, vr, vv, bst, bupd, sm, n, (int)F);
+      k_bi_beta<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, bupd, sm, S, (int)F, opt.psi_itmax, d_any); VSAV_COUNT_LAUNCH();
+      k_psi_p<T><<<gridfor(F * n), 256, 0, st>>>(vp, vr, vv, bst, bupd, sm, n, (int)F); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
       if (opt.check_every_iter) {
         VSAV_CUDA(cudaMemcpyAsync(h_pinned_any, d_any, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -637,9 +701,9 @@ class Solver : public SolverBase {
         if (!*h_pinned_any) break;
       }
       // refresh the activity flags for the operator kernels of the next iteration
-      k_bi_flags<<<(S + 63) / 64, 64, 0, st>>>(bst, bupd, S);
+      k_bi_flags<<<(S + 63) / 64, 64, 0, st>>>(bst, bupd, S); VSAV_COUNT_LAUNCH();
     }
-    if (full) { k_trunc<T><<<gridfor(F * g.Ny * g.kp), 256, 0, st>>>(vx, cache + 5 * VH, g.Nx, g.Ny, g.kp, g.nkx, (int)F); VSAV_LAUNCH_CHECK(); }
+    if (full) { k_trunc<T><<<gridfor(F * g.Ny * g.kp), 256, 0, st>>>(vx, cache + 5 * VH, g.Nx, g.Ny, g.kp, g.nkx, (int)F); VSAV_COUNT_LAUNCH(); VSAV_LAUNCH_CHECK(); }
   }
 
   // ------------------------------------------------------------------ host transfer
@@ -663,8 +727,8 @@ class Solver : public SolverBase {
     size_t nbytes = hat ? (size_t)Fo * Fi * rows * g.nkx * 16 : (size_t)Fo * Fi * g.P * 8;
     if (dir == 0) VSAV_CUDA(cudaMemcpyAsync(stage, host, nbytes, is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
     long long tot = hat ? (long long)Fo * Fi * rows * g.nkx : (long long)Fo * Fi * g.P;
-    if (hat) k_import_hat<T><<<gridfor(tot), 256, 0, st>>>(stage, (C*)dst, Fo, Fi, rows, g.nkx, g.kp, dir);
-    else k_import_real<T><<<gridfor(tot), 256, 0, st>>>(stage, (T*)dst, Fo, Fi, g.P, dir);
+    if (hat) { k_import_hat<T><<<gridfor(tot), 256, 0, st>>>(stage, (C*)dst, Fo, Fi, rows, g.nkx, g.kp, dir); VSAV_COUNT_LAUNCH(); }
+    else { k_import_real<T><<<gridfor(tot), 256, 0, st>>>(stage, (T*)dst, Fo, Fi, g.P, dir); VSAV_COUNT_LAUNCH(); }
     VSAV_LAUNCH_CHECK();
     if (dir == 1) VSAV_CUDA(cudaMemcpyAsync(host, stage, nbytes, cudaMemcpyDeviceToHost, st));
     VSAV_CUDA(cudaStreamSynchronize(st));
@@ -706,13 +770,13 @@ class Solver : public SolverBase {
     if (what == 0 || what == 1 || what == 2) {
       const C* src = what == 0 ? cache + idx * VH : (what == 1 ? s3 + idx * VH : uth + idx * nd * RH);
       int Fo = what == 2 ? R : V, Fi = what == 2 ? nd : 1;
-      k_import_hat<T><<<gridfor((long long)Fo * Fi * rows * g.nkx), 256, 0, st>>>(stage, (C*)src, Fo, Fi, rows, g.nkx, g.kp, 1);
+      k_import_hat<T><<<gridfor((long long)Fo * Fi * rows * g.nkx), 256, 0, st>>>(stage, (C*)src, Fo, Fi, rows, g.nkx, g.kp, 1); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
       VSAV_CUDA(cudaMemcpyAsync(host, stage, (size_t)Fo * Fi * rows * g.nkx * 16, cudaMemcpyDeviceToHost, st));
     } else {
       const T* src = what == 3 ? utp + idx * nd * RP : H4 + idx * VP;
       int Fo = what == 3 ? R : V, Fi = what == 3 ? nd : 1;
-      k_import_real<T><<<gridfor((long long)Fo * Fi * g.P), 256, 0, st>>>(stage, (T*)src, Fo, Fi, g.P, 1);
+      k_import_real<T><<<gridfor((long long)Fo * Fi * g.P), 256, 0, st>>>(stage, (T*)src, Fo, Fi, g.P, 1); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
       VSAV_CUDA(cudaMemcpyAsync(host, stage, (size_t)Fo * Fi * g.P * 8, cudaMemcpyDeviceToHost, st));
     }
@@ -749,17 +813,17 @@ class Solver : public SolverBase {
     C* hbuf = rhs;
     if (kind == 0) {
       VSAV_CUDA(cudaMemcpyAsync(stage, in, (size_t)nf * g.P * 8, cudaMemcpyDefault, st));
-      k_import_real<T><<<gridfor(nf * g.P), 256, 0, st>>>(stage, rbuf, nf, 1, g.P, 0);
+      k_import_real<T><<<gridfor(nf * g.P), 256, 0, st>>>(stage, rbuf, nf, 1, g.P, 0); VSAV_COUNT_LAUNCH();
       rfft(rbuf, nf, hbuf);
-      k_import_hat<T><<<gridfor(nf * rows * g.nkx), 256, 0, st>>>(stage, hbuf, nf, 1, rows, g.nkx, g.kp, 1);
+      k_import_hat<T><<<gridfor(nf * rows * g.nkx), 256, 0, st>>>(stage, hbuf, nf, 1, rows, g.nkx, g.kp, 1); VSAV_COUNT_LAUNCH();
       VSAV_CUDA(cudaMemcpyAsync(out, stage, (size_t)nf * rows * g.nkx * 16, cudaMemcpyDefault, st));
     } else {
       int mult = kind == 1 ? M_ONE : kind - 10;
       VSAV_CUDA(cudaMemcpyAsync(stage, in, (size_t)nf * rows * g.nkx * 16, cudaMemcpyDefault, st));
       VSAV_CUDA(cudaMemsetAsync(hbuf, 0, (size_t)nf * g.H * sizeof(C), st));
-      k_import_hat<T><<<gridfor(nf * rows * g.nkx), 256, 0, st>>>(stage, hbuf, nf, 1, rows, g.nkx, g.kp, 0);
+      k_import_hat<T><<<gridfor(nf * rows * g.nkx), 256, 0, st>>>(stage, hbuf, nf, 1, rows, g.nkx, g.kp, 0); VSAV_COUNT_LAUNCH();
       irfft(hbuf, nf, rbuf, mult);
-      k_import_real<T><<<gridfor(nf * g.P), 256, 0, st>>>(stage, rbuf, nf, 1, g.P, 1);
+      k_import_real<T><<<gridfor(nf * g.P), 256, 0, st>>>(stage, rbuf, nf, 1, g.P, 1); VSAV_COUNT_LAUNCH();
       VSAV_CUDA(cudaMemcpyAsync(out, stage, (size_t)nf * g.P * 8, cudaMemcpyDefault, st));
     }
     VSAV_LAUNCH_CHECK();
@@ -786,6 +850,18 @@ class Solver : public SolverBase {
     return s;
   }
   void sync() override { VSAV_CUDA(cudaStreamSynchronize(st)); }
+  void profile(int enable) override {
+    VSAV_CUDA(cudaStreamSynchronize(st));
+    if (enable == 2) { prof.reset(); return; }
+    prof.collect();
+    prof.enable(enable != 0);
+  }
+  void profile_read(int cls, double* out3) override {
+    VSAV_CUDA(cudaStreamSynchronize(st));
+    prof.collect();
+    out3[0] = (double)prof.launches[cls]; out3[1] = prof.ms[cls]; out3[2] = prof.bytes[cls];
+  }
+  cudaStream_t stream() override { return st; }
 };
 
 }  // namespace vsav

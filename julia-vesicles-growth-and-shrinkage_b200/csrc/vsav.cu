@@ -248,6 +248,39 @@ int vsav_get_scalar_work(vsav_handle* h, int32_t what, double* out) {
     return VSAV_OK;
   });
 }
+int vsav_time_run(vsav_handle* h, int32_t n0, int32_t nsteps, const double* dt, int32_t monitor, double* device_ms) {
+  return guard(h, [&] {
+    if (!device_ms) throw std::runtime_error("bad args");
+    cudaEvent_t a, b;
+    VSAV_CUDA(cudaEventCreate(&a));
+    VSAV_CUDA(cudaEventCreate(&b));
+    h->s->sync();
+    VSAV_CUDA(cudaEventRecord(a, h->s->stream()));
+    std::vector<double> e(monitor ? (size_t)nsteps * h->R : 0), ar(e.size());
+    int rc = vsav_run(h, n0, nsteps, dt, monitor ? e.data() : nullptr, monitor ? ar.data() : nullptr, nullptr);
+    VSAV_CUDA(cudaEventRecord(b, h->s->stream()));
+    VSAV_CUDA(cudaEventSynchronize(b));
+    float t = 0;
+    VSAV_CUDA(cudaEventElapsedTime(&t, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *device_ms = t;
+    return rc;
+  });
+}
+int64_t vsav_launch_count(void) { return (int64_t)launch_counter().load(); }
+
+int vsav_profile(vsav_handle* h, int32_t enable) {
+  return guard(h, [&] { h->s->profile(enable); return VSAV_OK; });
+}
+int vsav_profile_read(vsav_handle* h, int32_t kclass, double* out3) {
+  return guard(h, [&] {
+    if (!out3 || kclass < 0 || kclass >= KC_N) throw std::runtime_error("bad kernel class");
+    h->s->profile_read(kclass, out3);
+    return VSAV_OK;
+  });
+}
+
 int vsav_transform(vsav_handle* h, int32_t kind, int32_t nf, const double* in, double* out) {
   return guard(h, [&] {
     bool ok = in && out && nf >= 1 && nf <= 3 * h->V && (kind == 0 || kind == 1 || (kind >= 11 && kind <= 15));

@@ -14,6 +14,7 @@
 #include <cmath>
 #include <string>
 #include <stdexcept>
+#include <atomic>
 
 namespace vsav {
 
@@ -26,6 +27,10 @@ namespace vsav {
   } while (0)
 
 #define VSAV_LAUNCH_CHECK() VSAV_CUDA(cudaGetLastError())
+
+// number of kernels this library has launched (all handles, all threads)
+inline std::atomic<long long>& launch_counter() { static std::atomic<long long> c{0}; return c; }
+#define VSAV_COUNT_LAUNCH() (::vsav::launch_counter().fetch_add(1, std::memory_order_relaxed))
 
 template <typename T> struct CplxOf;
 template <> struct CplxOf<float> { using type = float2; };

@@ -22,7 +22,8 @@ EXPORTS = ("vsav_create", "vsav_destroy", "vsav_last_error", "vsav_create_error"
            "vsav_set_field", "vsav_get_field", "vsav_set_scalars", "vsav_get_scalars", "vsav_set_dt",
            "vsav_set_A0", "vsav_get_A0", "vsav_init_state", "vsav_step1", "vsav_step2", "vsav_step3",
            "vsav_step4", "vsav_step5", "vsav_step6", "vsav_step7", "vsav_update_state", "vsav_run",
-           "vsav_monitor", "vsav_get_work", "vsav_get_scalar_work", "vsav_transform")
+           "vsav_monitor", "vsav_get_work", "vsav_get_scalar_work", "vsav_transform", "vsav_time_run",
+           "vsav_profile", "vsav_profile_read", "vsav_launch_count")
 
 
 class VsavConfig(ct.Structure):
@@ -93,6 +94,10 @@ def load(path: str = LIB_PATH):
         "vsav_get_work": ([H, i32, i32, D], ct.c_int),
         "vsav_get_scalar_work": ([H, i32, D], ct.c_int),
         "vsav_transform": ([H, i32, i32, D, D], ct.c_int),
+        "vsav_time_run": ([H, i32, i32, D, i32, D], ct.c_int),
+        "vsav_profile": ([H, i32], ct.c_int),
+        "vsav_profile_read": ([H, i32, D], ct.c_int),
+        "vsav_launch_count": ([], ct.c_int64),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)

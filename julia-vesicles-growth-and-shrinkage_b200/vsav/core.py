@@ -201,6 +201,25 @@ class Handle:
         self._chk(rc)
         return (E, A) if monitor else None
 
+    def time_run(self, n0, nsteps, monitor=True):
+        """nsteps full steps timed on the device with CUDA events (ms)."""
+        ms = np.zeros(1)
+        self._chk(self.lib.vsav_time_run(self.h, n0, nsteps, None, int(monitor), L.dptr(ms)))
+        return float(ms[0])
+
+    KCLASS = ("fft_cols", "fft_rows_r2c", "fft_rows_c2r", "fft_rows_c2c", "psi_rows_fused", "psi_combine")
+
+    def profile(self, enable):
+        self._chk(self.lib.vsav_profile(self.h, {True: 1, False: 0, "reset": 2}[enable]))
+
+    def profile_read(self):
+        out = {}
+        for i, k in enumerate(self.KCLASS):
+            a = np.zeros(3)
+            self._chk(self.lib.vsav_profile_read(self.h, i, L.dptr(a)))
+            out[k] = dict(launches=int(a[0]), ms=float(a[1]), bytes=float(a[2]))
+        return out
+
     def monitor(self):
         E = np.empty(self.R)
         A = np.empty(self.R)

@@ -207,8 +207,9 @@ def update_state(dest: FieldState, src: FieldState) -> FieldState:
 # Operators (src/SpectralUtils.jl:36-118, src/SpectralUtils_3d.jl:36-124)
 # ---------------------------------------------------------------------------
 class Operators:
-    def __init__(self, cfg: Config, counter: Optional[OpCounter] = None):
+    def __init__(self, cfg: Config, counter: Optional[OpCounter] = None, workers: Optional[int] = None):
         self.cfg = cfg
+        self.workers = workers
         self.counter = counter or OpCounter()
         nd = cfg.ndim
         # 2*pi*rfftfreq(Nx, Nx/Lx): Nyquist POSITIVE (SpectralUtils.jl:42)
@@ -246,25 +247,36 @@ class Operators:
     def _nb(self, a, nd):
         return int(np.prod(a.shape[:-nd])) if a.ndim > nd else 1
 
+    # numpy.fft and scipy.fft are both pocketfft; scipy's takes a thread count
+    def _mod(self):
+        if self.workers:
+            import scipy.fft as sf
+            return sf, dict(workers=self.workers)
+        return np.fft, {}
+
     def rfft(self, f):
         self.counter.rfft += self._nb(f, self.cfg.ndim)
-        return np.fft.rfftn(f, axes=self.axes)
+        m, kw = self._mod()
+        return m.rfftn(f, axes=self.axes, **kw)
 
     def irfft(self, F):
         self.counter.irfft += self._nb(F, self.cfg.ndim)
-        return np.fft.irfftn(F, s=self.cfg.shape, axes=self.axes)
+        m, kw = self._mod()
+        return m.irfftn(F, s=self.cfg.shape, axes=self.axes, **kw)
 
     def fft(self, f):
         self.counter.cfft += self._nb(f, self.cfg.ndim)
-        return np.fft.fftn(f, axes=self.axes)
+        m, kw = self._mod()
+        return m.fftn(f, axes=self.axes, **kw)
 
     def ifft(self, F):
         self.counter.cfft += self._nb(F, self.cfg.ndim)
-        return np.fft.ifftn(F, axes=self.axes)
+        m, kw = self._mod()
+        return m.ifftn(F, axes=self.axes, **kw)
 
 
-def build_operators(cfg: Config, counter: Optional[OpCounter] = None) -> Operators:
-    return Operators(cfg, counter)
+def build_operators(cfg: Config, counter: Optional[OpCounter] = None, workers: Optional[int] = None) -> Operators:
+    return Operators(cfg, counter, workers)
 
 
 def mult(u_hat, v_hat, ops: Operators):
@@ -556,9 +568,9 @@ class Oracle:
     reference uses atol=1e-14, rtol=cfg.tol, itmax=20)."""
 
     def __init__(self, cfg: Config, psi_atol=1e-14, psi_rtol=None, psi_itmax=20,
-                 counter: Optional[OpCounter] = None):
+                 counter: Optional[OpCounter] = None, workers: Optional[int] = None):
         self.cfg = cfg
-        self.ops = build_operators(cfg, counter)
+        self.ops = build_operators(cfg, counter, workers)
         self.psi_atol = psi_atol
         self.psi_rtol = cfg.tol if psi_rtol is None else psi_rtol
         self.psi_itmax = psi_itmax

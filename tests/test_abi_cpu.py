@@ -14,7 +14,7 @@ HEADER = os.path.join(ROOT, "include", "vsav.h")
 
 def declared_functions():
     txt = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*(?:int|void|const char\*)\s+(vsav_\w+)\s*\(", txt, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|int64_t|void|const char\*)\s+(vsav_\w+)\s*\(", txt, re.M)))
 
 
 def test_header_declares_the_reference_entry_points():
