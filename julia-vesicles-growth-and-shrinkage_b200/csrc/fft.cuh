@@ -9,9 +9,10 @@
 //  * one CTA owns a tile of E*nthreads complex elements in shared memory:
 //    nl whole rows (x pass) or TW whole columns (y / z pass), so each pass over
 //    HBM reads and writes every element exactly once, coalesced;
-//  * inside the tile: Stockham autosort passes of radix 2..16; every thread
-//    stages its E elements of a pass in registers (read all, barrier, write
-//    all), so the transform is in place with one padded buffer;
+//  * inside the tile: thread t owns one radix-E butterfly (E elements spaced
+//    L/E apart), so the first and the last radix-E passes run in registers
+//    straight from / to global memory; the middle Stockham passes (radix <= 32)
+//    go through two padded shared-memory buffers (ping-pong, one barrier each);
 //  * real transforms use the half-length complex trick with the pre/post
 //    processing fused into the x pass; the c2r keeps only Re of the kx=0 and
 //    kx=Nx/2 bins, the FFTW/pocketfft convention the reference relies on;
@@ -30,121 +31,221 @@ namespace vsav {
 __host__ __device__ __forceinline__ int line_pitch(int L) { return L + (L >> 4) + 1; }
 __device__ __forceinline__ int sidx(int line, int LP, int e) { return line * LP + e + (e >> 4); }
 
-// in-register DFT of size R (power of two <= 16), radix-2 DIT on bit-reversed input
 template <int R> struct Log2 { static constexpr int v = (R <= 1) ? 0 : 1 + Log2<R / 2>::v; };
 
+// cos(2 pi m / 32), m = 0..8 (mathematical constants)
+__host__ __device__ constexpr double cos32(int m) {
+  return m == 0 ? 1.0 : m == 1 ? 0.98078528040323044913 : m == 2 ? 0.92387953251128675613 :
+         m == 3 ? 0.83146961230254523708 : m == 4 ? 0.70710678118654752440 : m == 5 ? 0.55557023301960222474 :
+         m == 6 ? 0.38268343236508977173 : m == 7 ? 0.19509032201612826785 : 0.0;
+}
+// multiply a by exp(-2 pi i m/32) (forward) or exp(+2 pi i m/32) (inverse), 0 <= m < 16
 template <typename C, bool INV>
-__device__ __forceinline__ C tw16(C a, int m) {
-  // multiply by exp(-+2 pi i m/16), m in [0,8)
-  const double c1 = 0.92387953251128675613, s1 = 0.38268343236508977173, h = 0.70710678118654752440;
-  double cr, ci;
-  switch (m) {
-    case 0: return a;
-    case 1: cr = c1; ci = s1; break;
-    case 2: cr = h; ci = h; break;
-    case 3: cr = s1; ci = c1; break;
-    case 4: { C r; if (INV) { r.x = -a.y; r.y = a.x; } else { r.x = a.y; r.y = -a.x; } return r; }
-    case 5: cr = -s1; ci = c1; break;
-    case 6: cr = -h; ci = h; break;
-    default: cr = -c1; ci = s1; break;
-  }
+__device__ __forceinline__ C tw32(C a, int m) {
+  if (m == 0) return a;
+  if (m == 8) { C r; if (INV) { r.x = -a.y; r.y = a.x; } else { r.x = a.y; r.y = -a.x; } return r; }
+  // cos and sin of 2 pi m / 32 from the first-octant table
+  const double c = (m < 8) ? cos32(m) : -cos32(16 - m);
+  const double sn = (m < 8) ? cos32(8 - m) : cos32(m - 8);
   using S = decltype(a.x);
-  S wr = (S)cr, wi = INV ? (S)ci : (S)(-ci);
+  S wr = (S)c, wi = INV ? (S)sn : (S)(-sn);
   C r; r.x = a.x * wr - a.y * wi; r.y = a.x * wi + a.y * wr; return r;
 }
+template <typename C, bool INV>
+__device__ __forceinline__ C tw16(C a, int m) { return tw32<C, INV>(a, 2 * m); }
 
+// In-register DFT of size R (power of two <= 32): in-place radix-2
+// decimation-in-frequency network (no temporaries), then the bit-reversal
+// permutation as a register renaming (all indices compile-time constants).
+__host__ __device__ constexpr int brev(int r, int lg) {
+  int o = 0;
+  for (int b = 0; b < lg; ++b) o |= ((r >> b) & 1) << (lg - 1 - b);
+  return o;
+}
 template <int R, bool INV, typename C>
 __device__ __forceinline__ void dft_reg(C* v) {
   constexpr int LG = Log2<R>::v;
-  C a[R];
 #pragma unroll
-  for (int i = 0; i < R; ++i) {
-    int rev = 0;
-#pragma unroll
-    for (int b = 0; b < LG; ++b) rev |= ((i >> b) & 1) << (LG - 1 - b);
-    a[rev] = v[i];
-  }
-#pragma unroll
-  for (int len = 2; len <= R; len <<= 1) {
+  for (int len = R; len >= 2; len >>= 1) {
+    const int h = len / 2;
 #pragma unroll
     for (int i = 0; i < R; i += len) {
 #pragma unroll
-      for (int j = 0; j < len / 2; ++j) {
-        C u = a[i + j];
-        C t = tw16<C, INV>(a[i + j + len / 2], j * (16 / len));
-        a[i + j] = u + t;
-        a[i + j + len / 2] = u - t;
+      for (int j = 0; j < h; ++j) {
+        C u = v[i + j], w = v[i + j + h];
+        v[i + j] = u + w;
+        v[i + j + h] = tw32<C, INV>(u - w, j * (32 / len));
       }
     }
   }
+  C t[R];
 #pragma unroll
-  for (int i = 0; i < R; ++i) v[i] = a[i];
+  for (int r = 0; r < R; ++r) t[r] = v[brev(r, LG)];
+#pragma unroll
+  for (int r = 0; r < R; ++r) v[r] = t[r];
 }
 
-// one Stockham pass of radix R over nl lines of length L held in smem
-template <int R, int E, bool INV, typename C>
-__device__ __forceinline__ void stockham_pass(C* s, int LP, int logL, int nl, int p, const C* __restrict__ tab) {
+// shared-memory layouts of a tile of nl lines of length L
+//  RowLay: line-major, padded (x pass: lines are contiguous rows)
+//  ColLay: element-major [e][nl] with the line index fastest -- the natural
+//          layout of a tile of nl consecutive columns, conflict-free when
+//          consecutive threads take consecutive lines
+struct RowLay {
+  int LP;
+  __device__ __forceinline__ int operator()(int line, int e) const { return sidx(line, LP, e); }
+  static constexpr bool line_fast = false;
+};
+struct ColLay {
+  int nl, loge;    // nl lines; one nl-wide pad row every 2^loge elements (bank spreading)
+  __device__ __forceinline__ int operator()(int line, int e) const { return (e + (e >> loge)) * nl + line; }
+  static constexpr bool line_fast = true;
+};
+__host__ __device__ __forceinline__ int col_tile_elems(int L, int TW, int loge) { return (L + (L >> loge)) * TW; }
+
+// one out-of-place Stockham pass of radix R: src -> dst (ping-pong buffers),
+// one butterfly at a time (R complex registers + twiddles), one barrier
+template <int R, int E, bool INV, typename C, typename Lay>
+__device__ __forceinline__ void stockham_pass(const C* src, C* dst, const Lay lay, int logL, int lognl, int p,
+                                              const C* __restrict__ tab) {
   constexpr int NB = E / R;
   constexpr int LGR = Log2<R>::v;
   const int logLR = logL - LGR;
   const int LR = 1 << logLR;
-  const int nbut = nl << logLR;
+  const int nbut = 1 << (lognl + logLR);
   const int nthr = blockDim.x, tid = threadIdx.x;
-  C v[NB][R];
-#pragma unroll
+#pragma unroll 1
   for (int q = 0; q < NB; ++q) {
     int b = q * nthr + tid;
     if (b < nbut) {
-      int line = b >> logLR, i = b & (LR - 1);
-#pragma unroll
-      for (int r = 0; r < R; ++r) v[q][r] = s[sidx(line, LP, i + r * LR)];
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int q = 0; q < NB; ++q) {
-    int b = q * nthr + tid;
-    if (b < nbut) {
-      int line = b >> logLR, i = b & (LR - 1);
+      int line, i;
+      if (Lay::line_fast) { line = b & ((1 << lognl) - 1); i = b >> lognl; }
+      else { line = b >> logLR; i = b & (LR - 1); }
       int k = i & (p - 1);
+      C v[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = src[lay(line, i + r * LR)];
       if (p > 1) {
 #pragma unroll
         for (int r = 1; r < R; ++r) {
           C w = __ldg(&tab[p * R + r * k]);
           if (INV) w.y = -w.y;
-          v[q][r] = v[q][r] * w;
+          v[r] = v[r] * w;
         }
       }
-      dft_reg<R, INV>(v[q]);
+      dft_reg<R, INV>(v);
       int o = (i - k) * R + k;
 #pragma unroll
-      for (int r = 0; r < R; ++r) s[sidx(line, LP, o + r * p)] = v[q][r];
+      for (int r = 0; r < R; ++r) dst[lay(line, o + r * p)] = v[r];
     }
   }
   __syncthreads();
 }
 
-// full FFT of nl lines (length L = 2^logL) in smem, all threads of the CTA
-template <int E, bool INV, typename C>
-__device__ __forceinline__ void smem_fft(C* s, int LP, int logL, int nl, const C* __restrict__ tab) {
-  constexpr int LOGE = Log2<E>::v;
-  const int npass = (logL + LOGE - 1) / LOGE;
-  const int base = logL / npass, extra = logL % npass;
-  int p = 1;
+// Generic middle passes (ping-pong): Stockham passes of radix <= E from span p
+// over `bits` bits, starting in buf[cur]; returns the buffer index holding the result.
+template <int E, bool INV, typename C, typename Lay>
+__device__ __forceinline__ int smem_passes(C* const (&buf)[2], int cur, const Lay lay, int logL, int lognl, int p, int bits,
+                                           const C* __restrict__ tab) {
+  constexpr int LOGE = Log2<E>::v < 5 ? Log2<E>::v : 5;
+  if (bits <= 0) return cur;
+  const int npass = (bits + LOGE - 1) / LOGE;
+  const int base = bits / npass, extra = bits % npass;
   for (int ip = 0; ip < npass; ++ip) {
     int lr = base + (ip < extra ? 1 : 0);
+    const C* src = buf[cur];
+    C* dst = buf[cur ^ 1];
     switch (lr) {
-      case 1: stockham_pass<2, E, INV>(s, LP, logL, nl, p, tab); break;
-      case 2: stockham_pass<4, E, INV>(s, LP, logL, nl, p, tab); break;
-      case 3: stockham_pass<8, E, INV>(s, LP, logL, nl, p, tab); break;
+      case 1: stockham_pass<2, E, INV>(src, dst, lay, logL, lognl, p, tab); break;
+      case 2: if constexpr (E >= 4) stockham_pass<4, E, INV>(src, dst, lay, logL, lognl, p, tab); break;
+      case 3: if constexpr (E >= 8) stockham_pass<8, E, INV>(src, dst, lay, logL, lognl, p, tab); break;
+      case 4: if constexpr (E >= 16) stockham_pass<16, E, INV>(src, dst, lay, logL, lognl, p, tab); break;
       default:
-        if constexpr (E >= 16) stockham_pass<16, E, INV>(s, LP, logL, nl, p, tab);
+        if constexpr (E >= 32) stockham_pass<32, E, INV>(src, dst, lay, logL, lognl, p, tab);
         break;
     }
+    cur ^= 1;
     p <<= lr;
   }
+  return cur;
 }
 
+// FFT of a tile of 2^lognl lines of length L = 2^logL in which thread t owns
+// butterfly (line, i), i < L/E, i.e. the E elements i + j*(L/E) of `line`.
+//  ENTRY_REG: the input is in v[] (else: already in buf[0], natural order);
+//  EXIT_REG:  the output is returned in v[] (else: left in smem, natural order,
+//             in the buffer whose index is returned).
+// With L >= E^2 the first and the last radix-E passes run in registers and
+// only the middle passes go through shared memory (ping-pong buffers).
+template <int E, bool INV, bool ENTRY_REG, bool EXIT_REG, typename C, typename Lay>
+__device__ __forceinline__ int tile_fft(C (&v)[E], C* const (&buf)[2], const Lay lay, int line, int i, bool active,
+                                        int logL, int lognl, const C* __restrict__ tab) {
+  constexpr int LOGE = Log2<E>::v;
+  const int LE = 1 << (logL - LOGE);
+  int cur = 0;
+  if (logL >= 2 * LOGE) {
+    int p = 1, bits = logL;
+    if (ENTRY_REG) {
+      if (active) {
+        dft_reg<E, INV>(v);
+#pragma unroll
+        for (int r = 0; r < E; ++r) buf[0][lay(line, i * E + r)] = v[r];
+      }
+      __syncthreads();
+      p = E; bits -= LOGE;
+    }
+    cur = smem_passes<E, INV>(buf, 0, lay, logL, lognl, p, bits - (EXIT_REG ? LOGE : 0), tab);
+    if (EXIT_REG) {
+      if (active) {
+        const C* s = buf[cur];
+#pragma unroll
+        for (int r = 0; r < E; ++r) v[r] = s[lay(line, i + r * LE)];
+        // last pass: radix E at span p = L/E, so k = i; twiddles exp(-+2 pi i r i / L)
+        if constexpr (E >= 16) {
+          // w^(r i) = w^(4 (r/4) i) * w^((r%4) i): 3 + E/4 - 1 table loads, 2-ulp products
+          C lo[4], hi[E / 4];
+#pragma unroll
+          for (int q = 1; q < 4; ++q) { lo[q] = __ldg(&tab[(1 << logL) + q * i]); if (INV) lo[q].y = -lo[q].y; }
+#pragma unroll
+          for (int q = 1; q < E / 4; ++q) { hi[q] = __ldg(&tab[(1 << logL) + 4 * q * i]); if (INV) hi[q].y = -hi[q].y; }
+#pragma unroll
+          for (int r = 1; r < E; ++r) {
+            C w = (r & 3) == 0 ? hi[r >> 2] : ((r >> 2) == 0 ? lo[r & 3] : hi[r >> 2] * lo[r & 3]);
+            v[r] = v[r] * w;
+          }
+        } else {
+#pragma unroll
+          for (int r = 1; r < E; ++r) {
+            C w = __ldg(&tab[(1 << logL) + r * i]);
+            if (INV) w.y = -w.y;
+            v[r] = v[r] * w;
+          }
+        }
+        dft_reg<E, INV>(v);
+      }
+    }
+  } else {
+    if (ENTRY_REG) {
+      if (active) {
+#pragma unroll
+        for (int j = 0; j < E; ++j) buf[0][lay(line, i + j * LE)] = v[j];
+      }
+      __syncthreads();
+    }
+    cur = smem_passes<E, INV>(buf, 0, lay, logL, lognl, 1, logL, tab);
+    if (EXIT_REG && active) {
+      const C* s = buf[cur];
+#pragma unroll
+      for (int r = 0; r < E; ++r) v[r] = s[lay(line, i + r * LE)];
+    }
+  }
+  return cur;
+}
+
+
+// minimum resident CTAs that the register budget must allow, per (E, NT)
+template <int E, int NT> struct MinB {
+  static constexpr int v = (NT >= 512) ? ((E <= 8) ? 2 : 1) : ((E <= 4) ? 4 : ((E <= 8) ? 3 : 2));
+};
 template <typename T> struct FFTCfg;
 template <> struct FFTCfg<float> { static constexpr int E = 16; static constexpr int CHUNK = 4096; };
 template <> struct FFTCfg<double> { static constexpr int E = 8; static constexpr int CHUNK = 2048; };
@@ -183,122 +284,155 @@ __device__ __forceinline__ void c2r_pre(C A, C Braw, C w, C& Zk, C& ZLk) {
 // x pass, real -> half spectrum.  in = a0*in0 [+ a1*in1]  (rows of Nx reals)
 // out rows have pitch kp (complex).  nrows = F*Nz*Ny.
 // ---------------------------------------------------------------------------
-template <typename T>
-__global__ void __launch_bounds__(256) k_rows_r2c(const T* __restrict__ in0, const T* __restrict__ in1,
-                                                  T a0, T a1, cplx<T>* __restrict__ out,
-                                                  int logL, int nl, long long nrows, int kp,
-                                                  const cplx<T>* __restrict__ tab) {
+// thread -> butterfly (line, i) of a row tile: line = tid / (L/E), i = tid % (L/E)
+template <int E>
+__device__ __forceinline__ void row_owner(int logL, int& line, int& i) {
+  constexpr int LOGE = Log2<E>::v;
+  const int logLE = logL - LOGE;
+  line = threadIdx.x >> logLE;
+  i = threadIdx.x & ((1 << logLE) - 1);
+}
+
+template <typename T, int E, int NT>
+__global__ void __launch_bounds__(NT, MinB<E, NT>::v) k_rows_r2c(const T* __restrict__ in0, const T* __restrict__ in1,
+                                                              T a0, T a1, cplx<T>* __restrict__ out,
+                                                              int logL, int lognl, long long nrows, int kp,
+                                                              const cplx<T>* __restrict__ tab) {
   using C = cplx<T>;
-  constexpr int E = FFTCfg<T>::E;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* s = reinterpret_cast<C*>(smraw);
-  const int L = 1 << logL, LP = line_pitch(L);
+  const int L = 1 << logL, LP = line_pitch(L), nl = 1 << lognl, LE = L / E;
   const long long row0 = (long long)blockIdx.x * nl;
-  const int nthr = blockDim.x;
-  const int total = nl * L;
-  const C* zin0 = reinterpret_cast<const C*>(in0) + row0 * L;
-  const C* zin1 = in1 ? reinterpret_cast<const C*>(in1) + row0 * L : nullptr;
-  for (int f = threadIdx.x; f < total; f += nthr) {
-    int line = f >> logL, e = f & (L - 1);
-    if (row0 + line >= nrows) continue;
-    C z = zin0[f];
-    if (zin1) { C y = zin1[f]; z.x = a0 * z.x + a1 * y.x; z.y = a0 * z.y + a1 * y.y; }
-    else if (a0 != (T)1) { z.x *= a0; z.y *= a0; }
-    s[sidx(line, LP, e)] = z;
+  const long long rows_left = nrows - row0;
+  int line, i;
+  row_owner<E>(logL, line, i);
+  const bool active = line < rows_left;
+  C v[E];
+  if (active) {
+    const C* z0 = reinterpret_cast<const C*>(in0) + (row0 + line) * L + i;
+    const C* z1 = in1 ? reinterpret_cast<const C*>(in1) + (row0 + line) * L + i : nullptr;
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      C z = z0[j * LE];
+      if (z1) { C y = z1[j * LE]; z.x = a0 * z.x + a1 * y.x; z.y = a0 * z.y + a1 * y.y; }
+      else if (a0 != (T)1) { z.x *= a0; z.y *= a0; }
+      v[j] = z;
+    }
   }
-  __syncthreads();
-  smem_fft<E, false>(s, LP, logL, nl, tab);
+  C* const buf[2] = {s, s + nl * LP};
+  const C* so = buf[tile_fft<E, false, true, false>(v, buf, RowLay{LP}, line, i, active, logL, lognl, tab)];
   const int half = L / 2 + 1;
-  for (int f = threadIdx.x; f < nl * half; f += nthr) {
-    int line = f / half, k = f - line * half;
-    long long row = row0 + line;
-    if (row >= nrows) continue;
-    C Zk = s[sidx(line, LP, k)];
-    C Zc = s[sidx(line, LP, (L - k) & (L - 1))];
+  for (int f = threadIdx.x; f < nl * half; f += blockDim.x) {
+    int ln = f / half, k = f - ln * half;
+    if (ln >= rows_left) continue;
+    C Zk = so[sidx(ln, LP, k)];
+    C Zc = so[sidx(ln, LP, (L - k) & (L - 1))];
     C w = __ldg(&tab[2 * L + k]);
     C Xk, XLk;
     r2c_post(Zk, Zc, w, Xk, XLk);
-    C* orow = out + row * kp;
+    C* orow = out + (row0 + ln) * kp;
     orow[k] = Xk;
     if (k != L - k) orow[L - k] = XLk;
   }
 }
 
-// ---------------------------------------------------------------------------
-// x pass, half spectrum -> real, scaled.  in rows pitch kp.
-// ---------------------------------------------------------------------------
-template <typename T>
-__global__ void __launch_bounds__(256) k_rows_c2r(const cplx<T>* __restrict__ in, T* __restrict__ out, T scale,
-                                                  int logL, int nl, long long nrows, int kp,
-                                                  const cplx<T>* __restrict__ tab) {
+// load a half-spectrum row block [nl][L+1] (pitch kp) into smem, keeping only
+// Re of the kx=0 and kx=Nx/2 bins, and apply the c2r pre-processing in place
+template <typename T, int E>
+__device__ __forceinline__ void load_c2r_tile(const cplx<T>* __restrict__ in, cplx<T>* s, cplx<T>* sN, long long row0,
+                                              long long rows_left, int logL, int lognl, int kp,
+                                              const cplx<T>* __restrict__ tab) {
   using C = cplx<T>;
-  constexpr int E = FFTCfg<T>::E;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  C* s = reinterpret_cast<C*>(smraw);
-  const int L = 1 << logL, LP = line_pitch(L);
-  C* sN = s + nl * LP;                           // the kx = Nx/2 bin of each line
-  const long long row0 = (long long)blockIdx.x * nl;
-  const int nthr = blockDim.x;
-  for (int f = threadIdx.x; f < nl * (L + 1); f += nthr) {
-    int line = f / (L + 1), k = f - line * (L + 1);
-    if (row0 + line >= nrows) continue;
-    C x = in[(row0 + line) * kp + k];
-    if (k == 0 || k == L) x.y = (T)0;           // c2r keeps Re of the DC and Nyquist bins
-    if (k == L) sN[line] = x; else s[sidx(line, LP, k)] = x;
+  const int L = 1 << logL, LP = line_pitch(L), nl = 1 << lognl, LE = L / E;
+  int line, i;
+  row_owner<E>(logL, line, i);
+  if (line < rows_left) {
+    C xl[E];
+    const C* src = in + (row0 + line) * kp + i;
+#pragma unroll
+    for (int j = 0; j < E; ++j) xl[j] = src[j * LE];
+    if (i == 0) xl[0].y = (T)0;                  // c2r keeps Re of the DC and Nyquist bins
+#pragma unroll
+    for (int j = 0; j < E; ++j) s[sidx(line, LP, i + j * LE)] = xl[j];
   }
+  for (int ln = threadIdx.x; ln < nl; ln += blockDim.x)
+    if (ln < rows_left) { C x = in[(row0 + ln) * kp + L]; x.y = (T)0; sN[ln] = x; }
   __syncthreads();
   const int half = L / 2 + 1;
-  for (int f = threadIdx.x; f < nl * half; f += nthr) {
-    int line = f / half, k = f - line * half;
-    C A = s[sidx(line, LP, k)];
-    C B = (k == 0) ? sN[line] : s[sidx(line, LP, L - k)];
+  for (int f = threadIdx.x; f < nl * half; f += blockDim.x) {
+    int ln = f / half, k = f - ln * half;
+    C A = s[sidx(ln, LP, k)];
+    C B = (k == 0) ? sN[ln] : s[sidx(ln, LP, L - k)];
     C w = __ldg(&tab[2 * L + k]);
     C Zk, ZLk;
     c2r_pre(A, B, w, Zk, ZLk);
-    s[sidx(line, LP, k)] = Zk;
-    if (k != 0 && k != L - k) s[sidx(line, LP, L - k)] = ZLk;
+    s[sidx(ln, LP, k)] = Zk;
+    if (k != 0 && k != L - k) s[sidx(ln, LP, L - k)] = ZLk;
   }
   __syncthreads();
-  smem_fft<E, true>(s, LP, logL, nl, tab);
-  C* zo = reinterpret_cast<C*>(out) + row0 * L;
-  for (int f = threadIdx.x; f < nl * L; f += nthr) {
-    int line = f >> logL, e = f & (L - 1);
-    if (row0 + line >= nrows) continue;
-    C z = s[sidx(line, LP, e)];
-    z.x *= scale; z.y *= scale;
-    zo[f] = z;
+}
+
+// ---------------------------------------------------------------------------
+// x pass, half spectrum -> real, scaled.  in rows pitch kp.
+// ---------------------------------------------------------------------------
+template <typename T, int E, int NT>
+__global__ void __launch_bounds__(NT, MinB<E, NT>::v) k_rows_c2r(const cplx<T>* __restrict__ in, T* __restrict__ out, T scale,
+                                                              int logL, int lognl, long long nrows, int kp,
+                                                              const cplx<T>* __restrict__ tab) {
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* s = reinterpret_cast<C*>(smraw);
+  const int L = 1 << logL, LP = line_pitch(L), nl = 1 << lognl, LE = L / E;
+  C* sN = s + 2 * nl * LP;
+  const long long row0 = (long long)blockIdx.x * nl;
+  const long long rows_left = nrows - row0;
+  load_c2r_tile<T, E>(in, s, sN, row0, rows_left, logL, lognl, kp, tab);
+  int line, i;
+  row_owner<E>(logL, line, i);
+  const bool active = line < rows_left;
+  C v[E];
+  C* const buf[2] = {s, s + nl * LP};
+  tile_fft<E, true, false, true>(v, buf, RowLay{LP}, line, i, active, logL, lognl, tab);
+  if (active) {
+    C* zo = reinterpret_cast<C*>(out) + (row0 + line) * L + i;
+#pragma unroll
+    for (int j = 0; j < E; ++j) { C z = v[j]; z.x *= scale; z.y *= scale; zo[j * LE] = z; }
   }
 }
 
 // ---------------------------------------------------------------------------
 // x pass, full complex rows (length L = Nx).  in_real: input is a real field.
 // ---------------------------------------------------------------------------
-template <typename T, bool INV>
-__global__ void __launch_bounds__(256) k_rows_c2c(const cplx<T>* __restrict__ in, const T* __restrict__ in_real,
-                                                  cplx<T>* __restrict__ out, T scale, int logL, int nl,
-                                                  long long nrows, const cplx<T>* __restrict__ tab) {
+template <typename T, int E, int NT, bool INV>
+__global__ void __launch_bounds__(NT, MinB<E, NT>::v) k_rows_c2c(const cplx<T>* __restrict__ in, const T* __restrict__ in_real,
+                                                              cplx<T>* __restrict__ out, T scale, int logL, int lognl,
+                                                              long long nrows, const cplx<T>* __restrict__ tab) {
   using C = cplx<T>;
-  constexpr int E = FFTCfg<T>::E;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* s = reinterpret_cast<C*>(smraw);
-  const int L = 1 << logL, LP = line_pitch(L);
+  const int L = 1 << logL, LP = line_pitch(L), nl = 1 << lognl, LE = L / E;
   const long long row0 = (long long)blockIdx.x * nl;
-  const int nthr = blockDim.x;
-  for (int f = threadIdx.x; f < nl * L; f += nthr) {
-    int line = f >> logL, e = f & (L - 1);
-    if (row0 + line >= nrows) continue;
-    C z;
-    if (in_real) { z.x = in_real[row0 * L + f]; z.y = (T)0; } else z = in[row0 * L + f];
-    s[sidx(line, LP, e)] = z;
+  const long long rows_left = nrows - row0;
+  int line, i;
+  row_owner<E>(logL, line, i);
+  const bool active = line < rows_left;
+  C v[E];
+  const long long off = (row0 + line) * L + i;
+  if (active) {
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      if (in_real) { v[j].x = in_real[off + j * LE]; v[j].y = (T)0; } else v[j] = in[off + j * LE];
+    }
   }
-  __syncthreads();
-  smem_fft<E, INV>(s, LP, logL, nl, tab);
-  for (int f = threadIdx.x; f < nl * L; f += nthr) {
-    int line = f >> logL, e = f & (L - 1);
-    if (row0 + line >= nrows) continue;
-    C z = s[sidx(line, LP, e)];
-    if (scale != (T)1) { z.x *= scale; z.y *= scale; }
-    out[row0 * L + f] = z;
+  C* const buf[2] = {s, s + nl * LP};
+  tile_fft<E, INV, true, true>(v, buf, RowLay{LP}, line, i, active, logL, lognl, tab);
+  if (active) {
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      C z = v[j];
+      if (scale != (T)1) { z.x *= scale; z.y *= scale; }
+      out[off + j * LE] = z;
+    }
   }
 }
 
@@ -312,7 +446,7 @@ __global__ void __launch_bounds__(256) k_rows_c2c(const cplx<T>* __restrict__ in
 //   2: 3D y pass (kx=c, ky=e, kz=o%Nz)   3: 2D full-spectrum y pass (kx=c in [0,Nx))
 // ---------------------------------------------------------------------------
 struct ColArgs {
-  int logL, S, W, TW, tiles;
+  int logL, S, W, TW, logTW, tiles;
   long long O;
   int kpv, nkv;      // validity: (c % kpv) < nkv
   int geo;
@@ -333,44 +467,51 @@ __device__ __forceinline__ C col_mult(const ColArgs& a, int mult, double ms, int
   return mult_value<C>(mult, kx * a.kxs, ky * a.kys, kz * a.kzs, ms);
 }
 
-template <typename T, bool INV>
-__global__ void __launch_bounds__(256) k_cols(const cplx<T>* __restrict__ in0, const cplx<T>* __restrict__ in1,
-                                              T a0, T a1, int mult, double mscale,
-                                              cplx<T>* __restrict__ out, T oscale, ColArgs a,
-                                              const cplx<T>* __restrict__ tab) {
+template <typename T, int E, int NT, bool INV>
+__global__ void __launch_bounds__(NT, MinB<E, NT>::v) k_cols(const cplx<T>* __restrict__ in0, const cplx<T>* __restrict__ in1,
+                                                          T a0, T a1, int mult, double mscale,
+                                                          cplx<T>* __restrict__ out, T oscale, ColArgs a,
+                                                          const cplx<T>* __restrict__ tab) {
   using C = cplx<T>;
-  constexpr int E = FFTCfg<T>::E;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* s = reinterpret_cast<C*>(smraw);
-  const int L = 1 << a.logL, LP = line_pitch(L);
+  const int L = 1 << a.logL, LE = L / E;
   const int tile = blockIdx.x % a.tiles;
   const long long o = blockIdx.x / a.tiles;
   const int c0 = tile * a.TW;
   const long long base = o * a.O + c0;
-  const int nthr = blockDim.x;
-  const int total = a.TW * L;
-  for (int f = threadIdx.x; f < total; f += nthr) {
-    int cl = f % a.TW, e = f / a.TW;
-    int c = c0 + cl;
-    C v = mk<C>(0.0, 0.0);
-    if (c < a.W && (c % a.kpv) < a.nkv) {
-      long long idx = base + (long long)e * a.S + cl;
-      v = in0[idx];
-      if (in1) { C y = in1[idx]; v.x = a0 * v.x + a1 * y.x; v.y = a0 * v.y + a1 * y.y; }
-      else if (a0 != (T)1) { v.x *= a0; v.y *= a0; }
-      if (mult != M_ONE) v = v * col_mult<C>(a, mult, mscale, c, e, o);
+  // thread -> column cl of the tile and butterfly i (elements i + j*L/E);
+  // the tile sits in smem in its global layout [e][TW]
+  const int cl = threadIdx.x & (a.TW - 1);
+  const int i = threadIdx.x >> a.logTW;
+  const int c = c0 + cl;
+  const bool valid = c < a.W && (c % a.kpv) < a.nkv;
+  const ColLay lay{a.TW, Log2<E>::v};
+  C v[E];
+  if (valid) {
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      long long idx = base + (long long)(i + j * LE) * a.S + cl;
+      v[j] = in0[idx];
+      if (in1) { C y = in1[idx]; v[j].x = a0 * v[j].x + a1 * y.x; v[j].y = a0 * v[j].y + a1 * y.y; }
     }
-    s[sidx(cl, LP, e)] = v;
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      if (!in1 && a0 != (T)1) { v[j].x *= a0; v[j].y *= a0; }
+      if (mult != M_ONE) v[j] = v[j] * col_mult<C>(a, mult, mscale, c, i + j * LE, o);
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < E; ++j) v[j] = mk<C>(0.0, 0.0);
   }
-  __syncthreads();
-  smem_fft<E, INV>(s, LP, a.logL, a.TW, tab);
-  for (int f = threadIdx.x; f < total; f += nthr) {
-    int cl = f % a.TW, e = f / a.TW;
-    int c = c0 + cl;
-    if (c < a.W && (c % a.kpv) < a.nkv) {
-      C v = s[sidx(cl, LP, e)];
-      if (oscale != (T)1) { v.x *= oscale; v.y *= oscale; }
-      out[base + (long long)e * a.S + cl] = v;
+  C* const buf[2] = {s, s + col_tile_elems(L, a.TW, Log2<E>::v)};
+  tile_fft<E, INV, true, true>(v, buf, lay, cl, i, true, a.logL, a.logTW, tab);
+  if (valid) {
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      C z = v[j];
+      if (oscale != (T)1) { z.x *= oscale; z.y *= oscale; }
+      out[base + (long long)(i + j * LE) * a.S + cl] = z;
     }
   }
 }

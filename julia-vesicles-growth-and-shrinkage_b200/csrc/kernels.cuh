@@ -173,23 +173,40 @@ __global__ void __launch_bounds__(256) k_surf(const T* __restrict__ phi, const T
   ew_store_partials<3>(acc, part, ew, sm);
 }
 
+// per-vesicle sum of the surface energy density f_surf (Utils.jl:36-42): the
+// single code path behind every area (A0 at initialisation, A in Steps 1/2),
+// so A - A0 is exactly 0 when phi is unchanged, as in the reference
+template <typename T>
+__global__ void __launch_bounds__(256) k_area(const T* __restrict__ phi, const T* __restrict__ gx, const T* __restrict__ gy,
+                                              Phys ph, EW ew, double2* part) {
+  __shared__ double sm[2 * 1 * 8];
+  KSum acc[1] = {{0, 0}};
+  const double e = ph.eps;
+  EW_LOOP(ew, f, i) {
+    long long j = (long long)f * ew.n + i;
+    double p = phi[j], x = gx[j], y = gy[j];
+    acc[0].add((3.0 * SQ2 / 4.0) * (g_(p) / e) + e * (x * x + y * y) / 2.0);
+  }
+  ew_store_partials<1>(acc, part, ew, sm);
+}
+
 // per-run SAV normalisers of the H functions (Utils.jl:159-206,228-248):
-//  fs[v*3+0..2] = (f_surf, f_bend, E2) sums, fo[v*3+1..2] = (f_osm, psi^2) sums,
+//  asum[v] = f_surf sums, fs[v*3+1..2] = (f_bend, E2) sums, fo[v*3+1..2] = (f_osm, psi^2) sums,
 //  Mmax_v[v] = block maxima.  Writes sc[r*8 + 0..7] = (R1s, R2s, R3s, Mmax, W1, W2, W3, -)
 //  and factor[v], area[v].  err |= 1/2/4 when W_i + C_i < 0.
-__global__ void k_fin_H(const double* __restrict__ fs, const double* __restrict__ fo, const double* __restrict__ mmax_v,
-                        const double* __restrict__ A0, Phys ph, Runs rn, double* __restrict__ sc,
+__global__ void k_fin_H(const double* __restrict__ asum, const double* __restrict__ fs, const double* __restrict__ fo,
+                        const double* __restrict__ mmax_v, const double* __restrict__ A0, Phys ph, Runs rn, double* __restrict__ sc,
                         double* __restrict__ factor, double* __restrict__ area, int* __restrict__ err) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= rn.R) return;
   double W1 = 0, Ssurf = 0, Sbend = 0, Se2 = 0, Sosm = 0, Spsi = 0, mm = -INFINITY;
   for (int v = rn.vbeg[r]; v < rn.vbeg[r + 1]; ++v) {
-    double A = fs[v * 3 + 0] * ph.cell;
+    double A = asum[v] * ph.cell;
     area[v] = A;
     double d = A - A0[v];
     W1 += 0.5 * ph.gamma_area * d * d;
     factor[v] = ph.gamma_area * d * (3.0 * SQ2 / 4.0);
-    Ssurf += fs[v * 3 + 0]; Sbend += fs[v * 3 + 1]; Se2 += fs[v * 3 + 2];
+    Ssurf += asum[v]; Sbend += fs[v * 3 + 1]; Se2 += fs[v * 3 + 2];
     Sosm += fo[v * 3 + 1]; Spsi += fo[v * 3 + 2];
     if (mmax_v) mm = fmax(mm, mmax_v[v]);
   }

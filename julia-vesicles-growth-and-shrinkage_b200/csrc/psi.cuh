@@ -44,87 +44,75 @@ struct SysMap {
 // nin consecutive field blocks (t1 | t2).  HALF rows: c2r/r2c of length Nx;
 // FULL rows: c2c of length Nx.
 // ---------------------------------------------------------------------------
-template <typename T, bool FULL>
-__global__ void __launch_bounds__(256) k_rows_mul(cplx<T>* __restrict__ t, const T* __restrict__ M, T mconst, T scale,
-                                                  int logL, int nl, long long nrows, int rowlen_c, int rows_per_field,
-                                                  SysMap sm, const int* __restrict__ active, const cplx<T>* __restrict__ tab) {
+template <typename T, int E, int NT, bool FULL>
+__global__ void __launch_bounds__(NT, MinB<E, NT>::v) k_rows_mul(cplx<T>* __restrict__ t, const T* __restrict__ M, T mconst, T scale,
+                                                              int logL, int lognl, long long nrows, int rowlen_c,
+                                                              int rows_per_field, SysMap sm, const int* __restrict__ active,
+                                                              int f0, int fc, const cplx<T>* __restrict__ tab) {
   using C = cplx<T>;
-  constexpr int E = FFTCfg<T>::E;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* s = reinterpret_cast<C*>(smraw);
-  const int L = 1 << logL, LP = line_pitch(L);
-  C* sN = s + nl * LP;
+  const int L = 1 << logL, LP = line_pitch(L), nl = 1 << lognl, LE = L / E;
+  C* sN = s + 2 * nl * LP;
+  C* const buf[2] = {s, s + nl * LP};
   const long long row0 = (long long)blockIdx.x * nl;
-  const int field = (int)(row0 / rows_per_field);
-  if (active && !active[sm.sys(field % (3 * sm.V))]) return;
-  const int v = field % sm.V;
-  const int nthr = blockDim.x;
+  // rows hold t1 | t2 of the fc chunk fields starting at global field f0
+  const int field = f0 + (int)(row0 / rows_per_field) % fc;
+  if (active && !active[sm.sys(field)]) return;
+  const int v_ = field % sm.V;
   const int Nx = FULL ? L : 2 * L;
-  // load
+  const long long rows_left = nrows - row0;
+  int line, i;
+  row_owner<E>(logL, line, i);
+  const bool act = line < rows_left;
+  const RowLay lay{LP};
+  C v[E];
+  // inverse x transform, result in registers (element i + j L/E of the row)
   if (FULL) {
-    for (int f = threadIdx.x; f < nl * L; f += nthr) {
-      int line = f >> logL, e = f & (L - 1);
-      if (row0 + line >= nrows) continue;
-      s[sidx(line, LP, e)] = t[(row0 + line) * rowlen_c + e];
+    if (act) {
+#pragma unroll
+      for (int j = 0; j < E; ++j) v[j] = t[(row0 + line) * rowlen_c + i + j * LE];
     }
+    tile_fft<E, true, true, true>(v, buf, lay, line, i, act, logL, lognl, tab);
   } else {
-    for (int f = threadIdx.x; f < nl * (L + 1); f += nthr) {
-      int line = f / (L + 1), k = f - line * (L + 1);
-      if (row0 + line >= nrows) continue;
-      C x = t[(row0 + line) * rowlen_c + k];
-      if (k == 0 || k == L) x.y = (T)0;
-      if (k == L) sN[line] = x; else s[sidx(line, LP, k)] = x;
-    }
-    __syncthreads();
-    const int half = L / 2 + 1;
-    for (int f = threadIdx.x; f < nl * half; f += nthr) {
-      int line = f / half, k = f - line * half;
-      C A = s[sidx(line, LP, k)];
-      C B = (k == 0) ? sN[line] : s[sidx(line, LP, L - k)];
-      C w = __ldg(&tab[2 * L + k]);
-      C Zk, ZLk;
-      c2r_pre(A, B, w, Zk, ZLk);
-      s[sidx(line, LP, k)] = Zk;
-      if (k != 0 && k != L - k) s[sidx(line, LP, L - k)] = ZLk;
+    load_c2r_tile<T, E>(t, s, sN, row0, rows_left, logL, lognl, rowlen_c, tab);
+    tile_fft<E, true, false, true>(v, buf, lay, line, i, act, logL, lognl, tab);
+  }
+  // multiply by M_psi of the row's vesicle (HALF: z[m] holds x[2m] + i x[2m+1])
+  if (act) {
+    const long long prow = (long long)v_ * rows_per_field + (row0 % rows_per_field) + line;
+    const T* Mr = M ? M + prow * (long long)Nx : nullptr;
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      int e = i + j * LE;
+      if (FULL) {
+        T m = (Mr ? Mr[e] : mconst) * scale;
+        v[j].x *= m; v[j].y *= m;
+      } else {
+        T m0 = (Mr ? Mr[2 * e] : mconst) * scale, m1 = (Mr ? Mr[2 * e + 1] : mconst) * scale;
+        v[j].x *= m0; v[j].y *= m1;
+      }
     }
   }
-  __syncthreads();
-  smem_fft<E, true>(s, LP, logL, nl, tab);
-  // multiply by M (real field) -- in HALF mode element z[m] holds x[2m] + i x[2m+1]
-  const long long prow0 = (long long)v * rows_per_field + (row0 % rows_per_field);
-  for (int f = threadIdx.x; f < nl * L; f += nthr) {
-    int line = f >> logL, e = f & (L - 1);
-    if (row0 + line >= nrows) continue;
-    const T* Mr = M ? M + (prow0 + line) * (long long)Nx : nullptr;
-    C z = s[sidx(line, LP, e)];
-    if (FULL) {
-      T m = (Mr ? Mr[e] : mconst) * scale;
-      z.x *= m; z.y *= m;
-    } else {
-      T m0 = (Mr ? Mr[2 * e] : mconst) * scale, m1 = (Mr ? Mr[2 * e + 1] : mconst) * scale;
-      z.x *= m0; z.y *= m1;
-    }
-    s[sidx(line, LP, e)] = z;
-  }
-  __syncthreads();
-  smem_fft<E, false>(s, LP, logL, nl, tab);
+  __syncthreads();   // smem is reused by the forward transform
   if (FULL) {
-    for (int f = threadIdx.x; f < nl * L; f += nthr) {
-      int line = f >> logL, e = f & (L - 1);
-      if (row0 + line >= nrows) continue;
-      t[(row0 + line) * rowlen_c + e] = s[sidx(line, LP, e)];
+    tile_fft<E, false, true, true>(v, buf, lay, line, i, act, logL, lognl, tab);
+    if (act) {
+#pragma unroll
+      for (int j = 0; j < E; ++j) t[(row0 + line) * rowlen_c + i + j * LE] = v[j];
     }
   } else {
+    const C* so = buf[tile_fft<E, false, true, false>(v, buf, lay, line, i, act, logL, lognl, tab)];
     const int half = L / 2 + 1;
-    for (int f = threadIdx.x; f < nl * half; f += nthr) {
-      int line = f / half, k = f - line * half;
-      if (row0 + line >= nrows) continue;
-      C Zk = s[sidx(line, LP, k)];
-      C Zc = s[sidx(line, LP, (L - k) & (L - 1))];
+    for (int f = threadIdx.x; f < nl * half; f += blockDim.x) {
+      int ln = f / half, k = f - ln * half;
+      if (ln >= rows_left) continue;
+      C Zk = so[sidx(ln, LP, k)];
+      C Zc = so[sidx(ln, LP, (L - k) & (L - 1))];
       C w = __ldg(&tab[2 * L + k]);
       C Xk, XLk;
       r2c_post(Zk, Zc, w, Xk, XLk);
-      C* orow = t + (row0 + line) * rowlen_c;
+      C* orow = t + (row0 + ln) * rowlen_c;
       orow[k] = Xk;
       if (k != L - k) orow[L - k] = XLk;
     }
@@ -174,10 +162,13 @@ __global__ void __launch_bounds__(256) k_psi_combine(const cplx<T>* __restrict__
                                                      const cplx<T>* __restrict__ cvec, const cplx<T>* __restrict__ svec,
                                                      int mode, const double* __restrict__ adt_r, const double* __restrict__ mmax_r,
                                                      double S4, VGeom g, SysMap sm, const int* __restrict__ active,
-                                                     EW ew, double2* part) {
+                                                     int f0, EW ew, double2* part) {
   __shared__ double smm[2 * 4 * 8];
   KSum acc[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
-  const int f = blockIdx.y;
+  // t1/t2 are chunk-local (field blockIdx.y of the chunk); x, y, c, s are global (field f0 + blockIdx.y)
+  const int f = f0 + blockIdx.y;
+  const long long tsh = ((long long)f - blockIdx.y) * g.n;    // global -> chunk-local slot shift
+  t1 -= tsh; t2 -= tsh;
   const int sy = sm.sys(f);
   const int r = sm.run_of[f % sm.V];
   const bool act = !active || active[sy];
@@ -217,7 +208,7 @@ __global__ void __launch_bounds__(256) k_psi_combine(const cplx<T>* __restrict__
       }
     }
   }
-  block_reduce_store<4>(acc, part + ((long long)blockIdx.y * ew.bpf + blockIdx.x) * 4, smm);
+  block_reduce_store<4>(acc, part + ((long long)f * ew.bpf + blockIdx.x) * 4, smm);
 }
 
 // r = M^-1 b, x = 0, p = r, dots <b, r>, ||r||^2  (Krylov.jl bicgstab initialisation)

@@ -9,6 +9,10 @@
 #include <vector>
 #include <memory>
 #include <algorithm>
+#include <type_traits>
+#include <cstdlib>
+#include <map>
+#include <mutex>
 #include "psi.cuh"
 
 namespace vsav {
@@ -78,9 +82,9 @@ __global__ void k_set_adt(const double* dt, double a, double* adt, int R) {
     if (r < R) adt[r] = a / dt[r];
   }
 
-__global__ void k_area0(const double* fd, double cell, double* A0, int V) {
+__global__ void k_area0(const double* asum, double cell, double* A0, int V) {
     int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v < V) A0[v] = fd[v * 3] * cell;
+    if (v < V) A0[v] = asum[v] * cell;
   }
 
 __global__ void k_init_scalars(const double* sch, double* s, int R) {
@@ -184,7 +188,7 @@ class Solver : public SolverBase {
   T *phis, *psis, *Mpsi, *ustar, *d4, *omega, *lapomega, *H4, *gG, *gstar, *adv;
   C *tmpH, *tmpH2, *Hh, *flh, *advh, *cache, *rhs, *s3, *uth;
   T *cphys, *mn, *gu, *gmu, *gnu, *conv, *coupl, *rhs2, *utp, *tmpP, *mon_lap, *mon_g4, *mon_ga, *mon_gp;
-  double *scH, *factor, *area, *mmax_v, *mmax_r, *fd, *fd2, *r2, *qv, *theta, *energy, *aratio;
+  double *scH, *factor, *area, *mmax_v, *mmax_r, *fd, *fd2, *r2, *qv, *theta, *energy, *aratio, *asum;
   double2* part;
   int* d_err;
   // psi solver
@@ -264,7 +268,7 @@ class Solver : public SolverBase {
     gnu = dalloc<T>(nd * VP); conv = dalloc<T>(nd * RP); coupl = dalloc<T>(nd * RP); rhs2 = dalloc<T>(nd * RP);
     utp = dalloc<T>(2 * nd * RP); tmpP = dalloc<T>(3 * VP);
     mon_lap = dalloc<T>(2 * VP); mon_g4 = dalloc<T>(4 * VP); mon_ga = dalloc<T>(2 * VP); mon_gp = dalloc<T>(2 * RP);
-    scH = dalloc<double>(8 * R); factor = dalloc<double>(V); area = dalloc<double>(V);
+    scH = dalloc<double>(8 * R); factor = dalloc<double>(V); area = dalloc<double>(V); asum = dalloc<double>(V);
     mmax_v = dalloc<double>(V); mmax_r = dalloc<double>(R);
     fd = dalloc<double>(3 * V * 32 + R * 32); fd2 = dalloc<double>(3 * V * 32 + R * 32);
     r2 = dalloc<double>(6 * R); qv = dalloc<double>(R); theta = dalloc<double>(2 * R);
@@ -285,6 +289,7 @@ class Solver : public SolverBase {
     stage_bytes = nh * sizeof(double);
     stage = dalloc<double>(nh);
     VSAV_CUDA(cudaStreamSynchronize(st));
+    autotune();
   }
 
   ~Solver() override {
@@ -307,47 +312,93 @@ class Solver : public SolverBase {
     VSAV_LAUNCH_CHECK();
   }
 
-  int rows_nl(int L, long long nrows, int cap_rows_per_field = 0) const {
-    int nl = std::max(1, FFTCfg<T>::CHUNK / L);
-    while (nl > 1 && nl / 2 >= nrows) nl /= 2;
-    if (cap_rows_per_field) while (nl > cap_rows_per_field) nl /= 2;
-    return nl;
+  // ---- FFT kernel variants: (E elements per thread, NT threads per CTA) ----
+  // The autotuner picks one variant per pass family at handle creation.
+  enum Fam { FAM_R2C = 0, FAM_C2R, FAM_C2C, FAM_MUL, FAM_COLS, FAM_N };
+  static constexpr int NVAR = 4;
+  static constexpr int VE[2][NVAR] = {{8, 8, 16, 32}, {4, 4, 8, 16}};      // [T==double][variant]
+  static constexpr int VNT[NVAR] = {256, 512, 256, 256};
+  int choice[FAM_N] = {0, 0, 0, 0, 0};
+  bool tuned_from_cache = false;
+  double tune_ms[FAM_N][NVAR] = {};
+  static constexpr int DIX = std::is_same<T, double>::value ? 1 : 0;
+  int vE(int v) const { return VE[DIX][v]; }
+
+  void area_sums(const T* phi, const T* gx, const T* gy, const EW& e) {
+    k_area<T><<<dim3(e.bpf, dm.V), 256, 0, st>>>(phi, gx, gy, ph, e, part); VSAV_COUNT_LAUNCH();
+    VSAV_LAUNCH_CHECK();
+    fin(1, dm.V, e, asum);
   }
-  size_t rows_smem(int L, int nl) const { return (size_t)(nl * line_pitch(L) + nl) * sizeof(C); }
+
+  int rows_lognl(int L, int E, int NT, long long nrows, int cap_rows = 0) const {
+    int nl = std::max(1, E * NT / L);
+    while (nl > 1 && nl / 2 >= nrows) nl /= 2;
+    if (cap_rows) while (nl > cap_rows) nl /= 2;
+    return ilog2(nl);
+  }
+  size_t rows_smem(int L, int nl) const { return (size_t)(2 * nl * line_pitch(L) + nl) * sizeof(C); }
+
+#define VSAV_DISPATCH(fam, ...)                                                          \
+  switch (choice[fam]) {                                                                 \
+    case 0: { constexpr int E_ = VE[DIX][0], NT_ = VNT[0]; __VA_ARGS__; } break;         \
+    case 1: { constexpr int E_ = VE[DIX][1], NT_ = VNT[1]; __VA_ARGS__; } break;         \
+    case 2: { constexpr int E_ = VE[DIX][2], NT_ = VNT[2]; __VA_ARGS__; } break;         \
+    default: { constexpr int E_ = VE[DIX][3], NT_ = VNT[3]; __VA_ARGS__; } break;        \
+  }
+
+  template <int E_, int NT_>
+  void set_smem_attr(const void* fn, size_t sm) {
+    if (sm > 48 * 1024) VSAV_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  }
 
   void rows_r2c(const T* in0, const T* in1, double a0, double a1, C* out, long long nrows) {
     int L = g.Nx / 2, logL = ilog2(L);
-    int nl = rows_nl(L, nrows);
-    int thr = std::max(32, nl * L / FFTCfg<T>::E);
-    long long grid = (nrows + nl - 1) / nl;
-    prof.begin(st);
-    k_rows_r2c<T><<<(unsigned)grid, thr, rows_smem(L, nl), st>>>(in0, in1, (T)a0, (T)a1, out, logL, nl, nrows, g.kp, tab); VSAV_COUNT_LAUNCH();
-    VSAV_LAUNCH_CHECK();
-    prof.end(st, KC_ROWS_R2C, (double)nrows * (g.Nx * sizeof(T) * (in1 ? 2 : 1) + g.nkx * sizeof(C)));
+    VSAV_DISPATCH(FAM_R2C, {
+      int lognl = rows_lognl(L, E_, NT_, nrows);
+      int nl = 1 << lognl;
+      int thr = std::max(1, nl * L / E_);
+      long long grid = (nrows + nl - 1) / nl;
+      size_t sm = rows_smem(L, nl);
+      set_smem_attr<E_, NT_>((const void*)k_rows_r2c<T, E_, NT_>, sm);
+      prof.begin(st);
+      k_rows_r2c<T, E_, NT_><<<(unsigned)grid, thr, sm, st>>>(in0, in1, (T)a0, (T)a1, out, logL, lognl, nrows, g.kp, tab);
+      VSAV_LAUNCH_CHECK();
+      prof.end(st, KC_ROWS_R2C, (double)nrows * (g.Nx * sizeof(T) * (in1 ? 2 : 1) + g.nkx * sizeof(C)));
+    })
   }
   void rows_c2r(const C* in, T* out, double scale, long long nrows) {
     int L = g.Nx / 2, logL = ilog2(L);
-    int nl = rows_nl(L, nrows);
-    int thr = std::max(32, nl * L / FFTCfg<T>::E);
-    long long grid = (nrows + nl - 1) / nl;
-    prof.begin(st);
-    k_rows_c2r<T><<<(unsigned)grid, thr, rows_smem(L, nl), st>>>(in, out, (T)scale, logL, nl, nrows, g.kp, tab); VSAV_COUNT_LAUNCH();
-    VSAV_LAUNCH_CHECK();
-    prof.end(st, KC_ROWS_C2R, (double)nrows * (g.Nx * sizeof(T) + g.nkx * sizeof(C)));
+    VSAV_DISPATCH(FAM_C2R, {
+      int lognl = rows_lognl(L, E_, NT_, nrows);
+      int nl = 1 << lognl;
+      int thr = std::max(1, nl * L / E_);
+      long long grid = (nrows + nl - 1) / nl;
+      size_t sm = rows_smem(L, nl);
+      set_smem_attr<E_, NT_>((const void*)k_rows_c2r<T, E_, NT_>, sm);
+      prof.begin(st);
+      k_rows_c2r<T, E_, NT_><<<(unsigned)grid, thr, sm, st>>>(in, out, (T)scale, logL, lognl, nrows, g.kp, tab);
+      VSAV_LAUNCH_CHECK();
+      prof.end(st, KC_ROWS_C2R, (double)nrows * (g.Nx * sizeof(T) + g.nkx * sizeof(C)));
+    })
   }
   template <bool INV>
   void rows_c2c(const C* in, const T* in_real, C* out, double scale, long long nrows) {
     int L = g.Nx, logL = ilog2(L);
-    int nl = rows_nl(L, nrows);
-    int thr = std::max(32, nl * L / FFTCfg<T>::E);
-    long long grid = (nrows + nl - 1) / nl;
-    prof.begin(st);
-    k_rows_c2c<T, INV><<<(unsigned)grid, thr, rows_smem(L, nl), st>>>(in, in_real, out, (T)scale, logL, nl, nrows, tab); VSAV_COUNT_LAUNCH();
-    VSAV_LAUNCH_CHECK();
-    prof.end(st, KC_ROWS_C2C, (double)nrows * g.Nx * ((in_real ? sizeof(T) : sizeof(C)) + sizeof(C)));
+    VSAV_DISPATCH(FAM_C2C, {
+      int lognl = rows_lognl(L, E_, NT_, nrows);
+      int nl = 1 << lognl;
+      int thr = std::max(1, nl * L / E_);
+      long long grid = (nrows + nl - 1) / nl;
+      size_t sm = rows_smem(L, nl);
+      set_smem_attr<E_, NT_>((const void*)k_rows_c2c<T, E_, NT_, INV>, sm);
+      prof.begin(st);
+      k_rows_c2c<T, E_, NT_, INV><<<(unsigned)grid, thr, sm, st>>>(in, in_real, out, (T)scale, logL, lognl, nrows, tab);
+      VSAV_LAUNCH_CHECK();
+      prof.end(st, KC_ROWS_C2C, (double)nrows * g.Nx * ((in_real ? sizeof(T) : sizeof(C)) + sizeof(C)));
+    })
   }
   // geo: 0 2D y (half), 1 3D z (half), 2 3D y (half), 3 2D y (full)
-  ColArgs colargs(int geo, long long& nouter) const {
+  ColArgs colargs(int geo, long long& nouter, int E, int NT) const {
     ColArgs a{};
     a.geo = geo; a.Nx = g.Nx; a.Ny = g.Ny; a.Nz = g.Nz; a.kp = g.kp;
     a.kxs = g.kxs; a.kys = g.kys; a.kzs = g.kzs;
@@ -357,28 +408,151 @@ class Solver : public SolverBase {
     else if (geo == 2) { L = g.Ny; a.S = g.kp; a.W = g.kp; a.O = (long long)g.Ny * g.kp; a.kpv = g.kp; a.nkv = g.nkx; nouter *= g.Nz; }
     else { L = g.Ny; a.S = g.Nx; a.W = g.Nx; a.O = (long long)g.Ny * g.Nx; a.kpv = g.Nx; a.nkv = g.Nx; }
     a.logL = ilog2(L);
-    int TW = std::max(1, FFTCfg<T>::CHUNK / L);
+    int TW = std::max(1, E * NT / L);
     while (TW > 1 && TW / 2 >= a.W) TW /= 2;
     a.TW = TW;
+    a.logTW = ilog2(TW);
     a.tiles = (a.W + TW - 1) / TW;
     return a;
   }
   void cols(bool inv, int geo, long long nf, const C* in0, const C* in1, double a0, double a1, int mult, double ms,
             C* out, double oscale) {
-    long long nouter = nf;
-    ColArgs a = colargs(geo, nouter);
-    int L = 1 << a.logL;
-    int thr = std::max(32, a.TW * L / FFTCfg<T>::E);
-    size_t sm = (size_t)(a.TW * line_pitch(L)) * sizeof(C);
-    long long grid = (long long)a.tiles * nouter;
-    long long valid_lines = (geo == 3) ? (long long)g.Nx : (long long)g.nkx * (geo == 1 ? g.Ny : 1);
-    double cb = (double)nouter * valid_lines * L * sizeof(C) * ((in1 ? 2 : 1) + 1);
-    prof.begin(st);
-    if (inv) { k_cols<T, true><<<(unsigned)grid, thr, sm, st>>>(in0, in1, (T)a0, (T)a1, mult, ms, out, (T)oscale, a, tab); VSAV_COUNT_LAUNCH(); }
-    else { k_cols<T, false><<<(unsigned)grid, thr, sm, st>>>(in0, in1, (T)a0, (T)a1, mult, ms, out, (T)oscale, a, tab); VSAV_COUNT_LAUNCH(); }
-    VSAV_LAUNCH_CHECK();
-    prof.end(st, KC_COLS, cb);
+    VSAV_DISPATCH(FAM_COLS, {
+      long long nouter = nf;
+      ColArgs a = colargs(geo, nouter, E_, NT_);
+      int L = 1 << a.logL;
+      int thr = std::max(a.TW, a.TW * L / E_);
+      size_t sm = 2 * (size_t)col_tile_elems(L, a.TW, ilog2(E_)) * sizeof(C);
+      long long grid = (long long)a.tiles * nouter;
+      long long valid_lines = (geo == 3) ? (long long)g.Nx : (long long)g.nkx * (geo == 1 ? g.Ny : 1);
+      double cb = (double)nouter * valid_lines * L * sizeof(C) * ((in1 ? 2 : 1) + 1);
+      prof.begin(st);
+      if (inv) {
+        set_smem_attr<E_, NT_>((const void*)k_cols<T, E_, NT_, true>, sm);
+        k_cols<T, E_, NT_, true><<<(unsigned)grid, thr, sm, st>>>(in0, in1, (T)a0, (T)a1, mult, ms, out, (T)oscale, a, tab);
+      } else {
+        set_smem_attr<E_, NT_>((const void*)k_cols<T, E_, NT_, false>, sm);
+        k_cols<T, E_, NT_, false><<<(unsigned)grid, thr, sm, st>>>(in0, in1, (T)a0, (T)a1, mult, ms, out, (T)oscale, a, tab);
+      }
+      VSAV_COUNT_LAUNCH();
+      VSAV_LAUNCH_CHECK();
+      prof.end(st, KC_COLS, cb);
+    })
   }
+  void rows_mul(C* t, long long nrows, bool full, int f0 = 0, int fc = 0) {
+    if (fc == 0) fc = (int)(nrows / (2 * g.Ny));
+    int L = full ? g.Nx : g.Nx / 2, logL = ilog2(L);
+    SysMap sm{dm.V, dm.R, d_run_of};
+    int rowlen = full ? g.Nx : g.kp;
+    VSAV_DISPATCH(FAM_MUL, {
+      int lognl = rows_lognl(L, E_, NT_, nrows, g.Ny);
+      int nl = 1 << lognl;
+      int thr = std::max(1, nl * L / E_);
+      long long grid = (nrows + nl - 1) / nl;
+      size_t smb = rows_smem(L, nl);
+      prof.begin(st);
+      if (full) {
+        set_smem_attr<E_, NT_>((const void*)k_rows_mul<T, E_, NT_, true>, smb);
+        k_rows_mul<T, E_, NT_, true><<<(unsigned)grid, thr, smb, st>>>(t, Mpsi, (T)0, (T)(1.0 / g.P), logL, lognl, nrows,
+                                                                       rowlen, g.Ny, sm, bupd, f0, fc, tab);
+      } else {
+        set_smem_attr<E_, NT_>((const void*)k_rows_mul<T, E_, NT_, false>, smb);
+        k_rows_mul<T, E_, NT_, false><<<(unsigned)grid, thr, smb, st>>>(t, Mpsi, (T)0, (T)(1.0 / g.P), logL, lognl, nrows,
+                                                                        rowlen, g.Ny, sm, bupd, f0, fc, tab);
+      }
+      VSAV_COUNT_LAUNCH();
+      VSAV_LAUNCH_CHECK();
+      // reads + writes t1|t2 rows and reads M once per row
+      prof.end(st, KC_ROWS_MUL, (double)nrows * ((full ? g.Nx : g.nkx) * 2.0 * sizeof(C) + g.Nx * sizeof(T)));
+    })
+  }
+
+  // time every variant of every pass family on scratch buffers; keep the fastest
+  // process-wide tuning cache: handles of the same shape reuse the first choice
+  static std::map<std::string, std::vector<int>>& tune_cache() { static std::map<std::string, std::vector<int>> m; return m; }
+  std::string tune_key() const {
+    return std::to_string(sizeof(T)) + ":" + std::to_string(g.Nx) + "x" + std::to_string(g.Ny) + "x" + std::to_string(g.Nz) +
+           ":V" + std::to_string(dm.V) + ":R" + std::to_string(dm.R) + ":f" + std::to_string(opt.psi_form);
+  }
+  bool variant_ok(int fam, int v) const {
+    int Lr = (fam == FAM_C2C || (fam == FAM_MUL && psi_full())) ? g.Nx : g.Nx / 2;
+    int Lc = (g.nd == 3) ? std::min(g.Ny, g.Nz) : g.Ny;
+    int L = (fam == FAM_COLS) ? Lc : Lr;
+    return vE(v) <= L && vE(v) * VNT[v] / L >= 1;
+  }
+  void autotune() {
+    if (const char* forced = getenv("VSAV_TUNE")) {      // "c0,c1,c2,c3,c4"
+      int k = 0;
+      for (const char* q = forced; *q && k < FAM_N; ++q)
+        if (*q >= '0' && *q <= '9') { int v = *q - '0'; if (v < NVAR && variant_ok(k, v)) choice[k] = v; ++k; }
+      return;
+    }
+    {
+      std::lock_guard<std::mutex> lk(tune_mutex());
+      auto it = tune_cache().find(tune_key());
+      if (it != tune_cache().end()) { for (int f = 0; f < FAM_N; ++f) choice[f] = it->second[f]; tuned_from_cache = true; return; }
+    }
+    autotune_measure();
+    std::lock_guard<std::mutex> lk(tune_mutex());
+    tune_cache()[tune_key()] = std::vector<int>(choice, choice + FAM_N);
+  }
+  static std::mutex& tune_mutex() { static std::mutex m; return m; }
+  void autotune_measure() {
+    cudaEvent_t e0, e1;
+    VSAV_CUDA(cudaEventCreate(&e0));
+    VSAV_CUDA(cudaEventCreate(&e1));
+    const int V = dm.V;
+    const long long nrows = (long long)V * g.Nz * g.Ny;
+    bool was = prof.on;
+    prof.on = false;
+    bool have_mul = (g.nd == 2) && vt12 != nullptr;
+    for (int fam = 0; fam < FAM_N; ++fam) {
+      if (fam == FAM_MUL && !have_mul) continue;
+      if (fam == FAM_C2C && !(g.nd == 2 && psi_full())) continue;
+      double best = 1e30;
+      int bestv = 0;
+      while (!variant_ok(fam, bestv) && bestv + 1 < NVAR) ++bestv;
+      for (int v = 0; v < NVAR; ++v) {
+        if (!variant_ok(fam, v)) continue;
+        choice[fam] = v;
+        auto run = [&]() {
+          switch (fam) {
+            case FAM_R2C: rows_r2c(tmpP, nullptr, 1, 0, tmpH, nrows); break;
+            case FAM_C2R: rows_c2r(tmpH, tmpP, 1.0, nrows); break;
+            case FAM_C2C: rows_c2c<false>(vb, nullptr, vt, 1.0, 3LL * V * g.Ny); break;
+            case FAM_MUL: rows_mul(vt12, 2LL * psi_chunk() * g.Ny, psi_full(), 0, psi_chunk()); break;
+            default: cols(false, g.nd == 2 ? 0 : 1, V, tmpH, nullptr, 1, 0, M_ONE, 1, tmpH, 1); break;
+          }
+        };
+        run();
+        VSAV_CUDA(cudaEventRecord(e0, st));
+        for (int k = 0; k < 3; ++k) run();
+        VSAV_CUDA(cudaEventRecord(e1, st));
+        VSAV_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        VSAV_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        tune_ms[fam][v] = ms / 3;
+        if (ms < best) { best = ms; bestv = v; }
+      }
+      choice[fam] = bestv;
+    }
+    prof.on = was;
+    if (getenv("VSAV_VERBOSE")) {
+      const char* nm[FAM_N] = {"rows_r2c", "rows_c2r", "rows_c2c", "rows_mul", "cols"};
+      for (int f = 0; f < FAM_N; ++f) for (int v = 0; v < NVAR; ++v) if (!variant_ok(f, v)) tune_ms[f][v] = -1;
+      for (int f = 0; f < FAM_N; ++f) {
+        fprintf(stderr, "[vsav autotune %s] %-9s", std::is_same<T, double>::value ? "fp64" : "fp32", nm[f]);
+        for (int v = 0; v < NVAR; ++v) fprintf(stderr, "  E%d/NT%d %.3f ms", vE(v), VNT[v], tune_ms[f][v]);
+        fprintf(stderr, "  -> %d\n", choice[f]);
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    // the scratch buffers carry garbage now: clear what later code expects zeroed
+    VSAV_CUDA(cudaMemsetAsync(tmpH, 0, std::max<long long>(8 * dm.V, 9 * dm.R) * g.H * sizeof(C), st));
+    VSAV_CUDA(cudaStreamSynchronize(st));
+  }
+
   // rfft over the nd spatial axes of nf real fields  (in = a0 in0 + a1 in1)
   void rfft(const T* in0, long long nf, C* out, const T* in1 = nullptr, double a0 = 1, double a1 = 0) {
     rows_r2c(in0, in1, a0, a1, out, nf * g.Nz * g.Ny);
@@ -421,10 +595,11 @@ class Solver : public SolverBase {
     irfft(tmpH2, V, d4 + VP, M_DY);
     irfft(tmpH2, V, d4 + 2 * VP, M_LAP);
     irfft(tmpH2, V, d4 + 3 * VP, M_BIH);
+    area_sums(phi, d4, d4 + VP, e);              // fd2 slot 0 of each vesicle <- f_surf sum
     k_surf<T><<<gv, 256, 0, st>>>(phi, d4, d4 + VP, d4 + 2 * VP, omega, ph, e, part); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     fin(3, V, e, fd);                                    // fd[v*3+0..2] = surf, bend, E2
-    k_fin_H<<<(dm.R + 63) / 64, 64, 0, st>>>(fd, fd2, star ? mmax_v : nullptr, d_A0, ph, rn, scH, factor, area, d_err); VSAV_COUNT_LAUNCH();
+    k_fin_H<<<(dm.R + 63) / 64, 64, 0, st>>>(asum, fd, fd2, star ? mmax_v : nullptr, d_A0, ph, rn, scH, factor, area, d_err); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     if (star) { k_copy_mmax<<<(dm.R + 63) / 64, 64, 0, st>>>(scH, mmax_r, dm.R); VSAV_COUNT_LAUNCH(); VSAV_LAUNCH_CHECK(); }
     rfft(omega, V, tmpH2);
@@ -596,10 +771,8 @@ class Solver : public SolverBase {
     rfft(phys4[0], V, tmpH2);
     irfft(tmpH2, V, mon_ga, M_DX);
     irfft(tmpH2, V, mon_ga + VP, M_DY);
-    k_surf<T><<<dim3(e.bpf, V), 256, 0, st>>>(phys4[0], mon_ga, mon_ga + VP, nullptr, nullptr, ph, e, part); VSAV_COUNT_LAUNCH();
-    VSAV_LAUNCH_CHECK();
-    fin(3, V, e, fd);
-    k_area0<<<(V + 63) / 64, 64, 0, st>>>(fd, ph.cell, d_A0, V); VSAV_COUNT_LAUNCH();
+    area_sums(phys4[0], mon_ga, mon_ga + VP, e);
+    k_area0<<<(V + 63) / 64, 64, 0, st>>>(asum, ph.cell, d_A0, V); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     compute_H(phys4[0], nullptr, phys4[0] + VP, nullptr, false);
     k_init_scalars<<<(R + 63) / 64, 64, 0, st>>>(scH, sc[0], R); VSAV_COUNT_LAUNCH();
@@ -616,46 +789,42 @@ class Solver : public SolverBase {
   }
 
   // ------------------------------------------------------------------ psi BiCGSTAB (2D)
+  // fields per chunk of the psi operator: the chunk's two intermediates stay in L2
+  // (chunking is off by default: VSAV_PSI_CHUNK_MB sets the L2 budget of a chunk)
+  int psi_chunk() const {
+    const char* env = getenv("VSAV_PSI_CHUNK_MB");
+    if (!env) return 3 * dm.V;
+    const long long per = 2LL * psi_n() * (long long)sizeof(C);
+    long long fc = std::max<long long>(1, (atoll(env) << 20) / per);
+    return (int)std::min<long long>(fc, 3LL * dm.V);
+  }
+
+  // y = P^-1 A in (+ dots), chunk by chunk: y-inverse (2 multipliers), fused
+  // x pass (inverse, x M_psi, forward), y-forward, combine
   void matvec(const C* in, C* out, int mode, const C* svec) {
     const int V = dm.V;
     const long long F = 3LL * V, n = psi_n();
     const bool full = psi_full();
-    C* t1 = vt12;
-    C* t2 = vt12 + F * n;
-    int geo = full ? 3 : 0;
-    cols(true, geo, F, in, nullptr, 1, 0, full ? M_DX0 : M_DXZ, ph.S4, t1, 1);
-    cols(true, geo, F, in, nullptr, 1, 0, M_DY, ph.S4, t2, 1);
-    // fused x pass on t1|t2
-    {
-      int L = full ? g.Nx : g.Nx / 2, logL = ilog2(L);
-      long long nrows = 2 * F * g.Ny;
-      int nl = rows_nl(L, nrows, g.Ny);
-      int thr = std::max(32, nl * L / FFTCfg<T>::E);
-      long long grid = (nrows + nl - 1) / nl;
-      SysMap sm{V, dm.R, d_run_of};
-      int rowlen = full ? g.Nx : g.kp;
-      prof.begin(st);
-      if (full) {
-        k_rows_mul<T, true><<<(unsigned)grid, thr, rows_smem(L, nl), st>>>(t1, Mpsi, (T)0, (T)(1.0 / g.P), logL, nl, nrows,
-                                                                           rowlen, g.Ny, sm, bupd, tab); VSAV_COUNT_LAUNCH();
-      } else {
-        k_rows_mul<T, false><<<(unsigned)grid, thr, rows_smem(L, nl), st>>>(t1, Mpsi, (T)0, (T)(1.0 / g.P), logL, nl, nrows,
-                                                                            rowlen, g.Ny, sm, bupd, tab); VSAV_COUNT_LAUNCH();
-      }
-      VSAV_LAUNCH_CHECK();
-      // reads+writes t1|t2 rows and reads M once per row (2F rows)
-      prof.end(st, KC_ROWS_MUL, (double)nrows * ((full ? g.Nx : g.nkx) * 2.0 * sizeof(C) + g.Nx * sizeof(T)));
-    }
-    cols(false, geo, 2 * F, t1, nullptr, 1, 0, M_ONE, 1, t1, 1);
+    const int geo = full ? 3 : 0;
+    const int Fc = psi_chunk();
     EW e = ew(n);
     VGeom vg{full ? 1 : 0, g.Nx, g.Ny, g.kp, g.nkx, n, g.kxs, g.kys};
     SysMap sm{V, dm.R, d_run_of};
     const double* pre = (opt.psi_precond >= 0) ? mmax_r : nullptr;
-    prof.begin(st);
-    k_psi_combine<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(in, t1, t2, out, vb, svec, mode, d_adt, pre, ph.S4, vg, sm,
-                                                                bupd, e, part); VSAV_COUNT_LAUNCH();
-    VSAV_LAUNCH_CHECK();
-    prof.end(st, KC_PSI_VEC, (double)F * (full ? g.Pfull : (long long)g.Ny * g.nkx) * 5.0 * sizeof(C));
+    for (int f0 = 0; f0 < F; f0 += Fc) {
+      const int fc = (int)std::min<long long>(Fc, F - f0);
+      C* t1 = vt12;
+      C* t2 = vt12 + (long long)fc * n;
+      cols(true, geo, fc, in + f0 * n, nullptr, 1, 0, full ? M_DX0 : M_DXZ, ph.S4, t1, 1);
+      cols(true, geo, fc, in + f0 * n, nullptr, 1, 0, M_DY, ph.S4, t2, 1);
+      rows_mul(t1, 2LL * fc * g.Ny, full, f0, fc);
+      cols(false, geo, 2LL * fc, t1, nullptr, 1, 0, M_ONE, 1, t1, 1);
+      prof.begin(st);
+      k_psi_combine<T><<<dim3(e.bpf, (unsigned)fc), 256, 0, st>>>(in, t1, t2, out, vb, svec, mode, d_adt, pre, ph.S4, vg,
+                                                                   sm, bupd, f0, e, part); VSAV_COUNT_LAUNCH();
+      VSAV_LAUNCH_CHECK();
+      prof.end(st, KC_PSI_VEC, (double)fc * (full ? g.Pfull : (long long)g.Ny * g.nkx) * 5.0 * sizeof(C));
+    }
   }
 
   void psi_solve() {

@@ -31,12 +31,19 @@ def params(eps: float, N: int, psi_in, psi_out, dt: float, T: float, Nx: int, Ny
     set_para_base coefficients (Init.jl:40-68) at the given eps."""
     gb = 0.1
     gin = gout = 1e5
+    S3 = gb / eps ** 3
+    # The SAV constant C2 must keep W2 + C2 > 0 (Utils.jl:180).  W2 contains
+    # -E2 ~ -S3/2 * int(phi^2) ~ -S3/2 * N |Omega|; the reference's C2 = 5e5
+    # (Init.jl:63) is sized for its unit box with one vesicle.  Keep it where it
+    # suffices and scale it (5x margin) otherwise.
+    area = L ** (3 if Nz else 2)
+    C2 = max(5.0e5, 5.0 * 0.5 * S3 * N * area)
     return dict(
         N=N, epsilon=eps, M_phi=1.0, M0_psi=0.5, eta=1.0, gamma_surf=1.0, gamma_area=5e4,
         gamma_bend=gb, gamma_in=gin, beta_in=0.0, psi_in_v=list(map(float, psi_in)),
         gamma_out=gout, beta_out=0.0, psi_out_v=list(map(float, psi_out)), lamda=1.0,
-        S1=(3 * SQ2 / 8) * eps * gb, S2=0.0, S3=gb / eps ** 3, S4=min(gin, gout),
-        C1=1.0, C2=5.0e5, C3=1.0e6, dt=dt, T=T, Nx=Nx, Ny=Ny, Lx=L, Ly=L, tol=tol, goal=goal,
+        S1=(3 * SQ2 / 8) * eps * gb, S2=0.0, S3=S3, S4=min(gin, gout),
+        C1=1.0, C2=C2, C3=1.0e6, dt=dt, T=T, Nx=Nx, Ny=Ny, Lx=L, Ly=L, tol=tol, goal=goal,
         Nz=Nz, Lz=(L if Nz else 0.0))
 
 
