@@ -124,14 +124,15 @@ __global__ void __launch_bounds__(NT, MinB<E, NT>::v) k_rows_mul(cplx<T>* __rest
 // ---------------------------------------------------------------------------
 struct VGeom {
   int full;         // 1 = FULL
-  int Nx, Ny, kp, nkx;
+  int Nx, Ny, kp, nkx, logNx;
   long long n;      // slots per field
   double kxs, kys;
 };
 __device__ __forceinline__ void vk(const VGeom& g, long long s, int& kx, int& ky, double& kxv, double& kyv, double& w) {
-  int rl = g.full ? g.Nx : g.kp;
-  kx = (int)(s % rl);
-  ky = (int)(s / rl);
+  // slot < 2^31 within a field: 32-bit index arithmetic (row lengths are powers of two or kp)
+  const unsigned su = (unsigned)s;
+  if (g.full) { kx = (int)(su & (unsigned)(g.Nx - 1)); ky = (int)(su >> g.logNx); }
+  else { ky = (int)(su / (unsigned)g.kp); kx = (int)(su - (unsigned)ky * (unsigned)g.kp); }
   kyv = kfreq(ky, g.Ny) * g.kys;
   if (g.full) { kxv = kfreq(kx, g.Nx) * g.kxs; w = 1.0; }
   else {
@@ -245,13 +246,12 @@ __global__ void __launch_bounds__(256) k_psi_init(const cplx<T>* __restrict__ b,
 // s = r - alpha v
 template <typename T>
 __global__ void k_psi_s(const cplx<T>* __restrict__ r, const cplx<T>* __restrict__ v, cplx<T>* __restrict__ s,
-                        const BiState* __restrict__ st, SysMap sm, long long n, int F) {
-  const long long tot = n * F;
-  K_LOOP(tot, i) {
-    int f = (int)(i / n);
-    const BiState& b = st[sm.sys(f)];
-    if (!b.active) continue;
-    double2 a = b.alpha;
+                        const BiState* __restrict__ st, SysMap sm, EW ew) {
+  const BiState& b = st[sm.sys(blockIdx.y)];
+  if (!b.active) return;
+  const double2 a = b.alpha;
+  EW_LOOP(ew, f, q) {
+    long long i = (long long)f * ew.n + q;
     cplx<T> rv = r[i], vv = v[i];
     cplx<T> o;
     o.x = (double)rv.x - (a.x * (double)vv.x - a.y * (double)vv.y);
@@ -302,14 +302,12 @@ __global__ void __launch_bounds__(256) k_psi_update(cplx<T>* __restrict__ x, cpl
 // p = r + beta (p - omega v)   (only systems that were active in this iteration: flag `upd`)
 template <typename T>
 __global__ void k_psi_p(cplx<T>* __restrict__ p, const cplx<T>* __restrict__ r, const cplx<T>* __restrict__ v,
-                        const BiState* __restrict__ st, const int* __restrict__ upd, SysMap sm, long long n, int F) {
-  const long long tot = n * F;
-  K_LOOP(tot, i) {
-    int f = (int)(i / n);
-    int sy = sm.sys(f);
-    if (!upd[sy]) continue;
-    const BiState& b = st[sy];
-    double2 be = b.beta, om = b.omega;
+                        const BiState* __restrict__ st, const int* __restrict__ upd, SysMap sm, EW ew) {
+  const int sy = sm.sys(blockIdx.y);
+  if (!upd[sy]) return;
+  const double2 be = st[sy].beta, om = st[sy].omega;
+  EW_LOOP(ew, f, q) {
+    long long i = (long long)f * ew.n + q;
     cplx<T> pv = p[i], rv = r[i], vv = v[i];
     double ax = (double)pv.x - (om.x * (double)vv.x - om.y * (double)vv.y);
     double ay = (double)pv.y - (om.x * (double)vv.y + om.y * (double)vv.x);

@@ -808,7 +808,7 @@ class Solver : public SolverBase {
     const int geo = full ? 3 : 0;
     const int Fc = psi_chunk();
     EW e = ew(n);
-    VGeom vg{full ? 1 : 0, g.Nx, g.Ny, g.kp, g.nkx, n, g.kxs, g.kys};
+    VGeom vg{full ? 1 : 0, g.Nx, g.Ny, g.kp, g.nkx, ilog2(g.Nx), n, g.kxs, g.kys};
     SysMap sm{V, dm.R, d_run_of};
     const double* pre = (opt.psi_precond >= 0) ? mmax_r : nullptr;
     for (int f0 = 0; f0 < F; f0 += Fc) {
@@ -841,7 +841,7 @@ class Solver : public SolverBase {
     }
     C* x = full ? vx : cache + 5 * VH;
     EW e = ew(n);
-    VGeom vg{full ? 1 : 0, g.Nx, g.Ny, g.kp, g.nkx, n, g.kxs, g.kys};
+    VGeom vg{full ? 1 : 0, g.Nx, g.Ny, g.kp, g.nkx, ilog2(g.Nx), n, g.kxs, g.kys};
     SysMap sm{V, R, d_run_of};
     k_psi_init<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(vb, x, vr, vp, d_adt, mmax_r, ph.S4, vg, sm, e, part); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
@@ -852,7 +852,7 @@ class Solver : public SolverBase {
       matvec(vp, vv, 0, nullptr);                       // v = M^-1 A p ; <c, v>
       fin(4, (int)F, e, fd);
       k_bi_alpha<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, sm, S, (int)F); VSAV_COUNT_LAUNCH();
-      k_psi_s<T><<<gridfor(F * n), 256, 0, st>>>(vr, vv, vs, bst, sm, n, (int)F); VSAV_COUNT_LAUNCH();
+      k_psi_s<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(vr, vv, vs, bst, sm, e); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
       matvec(vs, vt, 1, vs);                            // t = M^-1 A s ; <t,s>, <t,t>
       fin(4, (int)F, e, fd);
@@ -862,7 +862,7 @@ class Solver : public SolverBase {
       fin(4, (int)F, e, fd);
       VSAV_CUDA(cudaMemsetAsync(d_any, 0, sizeof(int), st));
       k_bi_beta<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, bupd, sm, S, (int)F, opt.psi_itmax, d_any); VSAV_COUNT_LAUNCH();
-      k_psi_p<T><<<gridfor(F * n), 256, 0, st>>>(vp, vr, vv, bst, bupd, sm, n, (int)F); VSAV_COUNT_LAUNCH();
+      k_psi_p<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(vp, vr, vv, bst, bupd, sm, e); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
       if (opt.check_every_iter) {
         VSAV_CUDA(cudaMemcpyAsync(h_pinned_any, d_any, sizeof(int), cudaMemcpyDeviceToHost, st));
