@@ -158,6 +158,27 @@ int vsav_get_scalar_work(vsav_handle* h, int32_t what, double* out);
  * (m: 1 D1x, 2 D1y, 3 D1z, 4 Laplacian, 5 Biharmonic).  nf <= 3 V. */
 int vsav_transform(vsav_handle* h, int32_t kind, int32_t nf, const double* in, double* out);
 
+/* No counterpart in the reference (an addition of this library).
+ * Inverse 2D real FFT in FP32 that allocates nothing, for callers that cannot
+ * call cudaMalloc -- code embedded in a host application that owns all GPU
+ * memory (a pool or arena), or that runs where a device allocation would
+ * block or is forbidden.  spec: device [nf][Ny][Nx/2+1] complex float
+ * (interleaved), out: device [nf][Ny][Nx] float; mult as in vsav_transform
+ * (0 none, 1 d/dx, 2 d/dy, 4 Laplacian, 5 biharmonic) with wavenumbers from
+ * Lx, Ly; stream: a cudaStream_t or NULL.  The one intermediate buffer lives
+ * in a fixed file-scope device array of 8 MiB (1 Mi complex floats) that every
+ * GPU holds from library load until process exit: nf * Ny * (Nx/2+1) above
+ * that limit is rejected with VSAV_E_INVALID (split the batch), as are Nx or
+ * Ny that are not powers of two up to 2048.  The first call on a device
+ * resolves that array's device address and uploads the twiddle table
+ * (synchronously), so make it before any stream capture.  All calls share the
+ * array: calls that can overlap on the GPU (different streams, devices'
+ * threads racing on one device) race; serialise them.  The error text of a
+ * failed call is returned by vsav_noalloc_error(). */
+int vsav_irfft2d_f32_noalloc(const float* spec, float* out, int32_t nf, int32_t Nx, int32_t Ny, double Lx,
+                             double Ly, int32_t mult, void* stream);
+const char* vsav_noalloc_error(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -29,7 +29,7 @@ def up_to_date():
 def build(force=False, verbose=True):
     if not force and up_to_date():
         return OUT
-    cmd = [NVCC] + FLAGS + ["-o", OUT + ".tmp", os.path.join(SRC, "vsav.cu")]
+    cmd = [NVCC] + FLAGS + ["-o", OUT + ".tmp", os.path.join(SRC, "vsav.cu"), os.path.join(SRC, "noalloc.cu")]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)

@@ -23,7 +23,8 @@ EXPORTS = ("vsav_create", "vsav_destroy", "vsav_last_error", "vsav_create_error"
            "vsav_set_A0", "vsav_get_A0", "vsav_init_state", "vsav_step1", "vsav_step2", "vsav_step3",
            "vsav_step4", "vsav_step5", "vsav_step6", "vsav_step7", "vsav_update_state", "vsav_run",
            "vsav_monitor", "vsav_get_work", "vsav_get_scalar_work", "vsav_transform", "vsav_time_run",
-           "vsav_profile", "vsav_profile_read", "vsav_launch_count")
+           "vsav_profile", "vsav_profile_read", "vsav_launch_count",
+           "vsav_irfft2d_f32_noalloc", "vsav_noalloc_error")
 
 
 class VsavConfig(ct.Structure):
@@ -98,6 +99,9 @@ def load(path: str = LIB_PATH):
         "vsav_profile": ([H, i32], ct.c_int),
         "vsav_profile_read": ([H, i32, D], ct.c_int),
         "vsav_launch_count": ([], ct.c_int64),
+        "vsav_irfft2d_f32_noalloc": ([ct.c_void_p, ct.c_void_p, i32, i32, i32, ct.c_double, ct.c_double, i32,
+                                      ct.c_void_p], ct.c_int),
+        "vsav_noalloc_error": ([], ct.c_char_p),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
