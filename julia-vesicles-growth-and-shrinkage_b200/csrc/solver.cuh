@@ -26,6 +26,9 @@ struct Options {
   int psi_itmax = 20;
   double psi_rtol = 1e-12, psi_atol = 1e-14;
   int check_every_iter = 1;  // read back convergence flags each BiCGSTAB iteration
+  int psi_mixed = 0;         // FP64 fields with the psi BiCGSTAB in FP32 + FP64 iterative refinement
+  int psi_refine = 2;        // refinement sweeps of the mixed mode
+  double psi_inner_rtol = 1e-6;
 };
 
 struct StepStatus {
@@ -166,6 +169,29 @@ struct Prof {
   ~Prof() { for (auto& x : ev) cudaEventDestroy(x); }
 };
 
+template <typename B> __device__ __forceinline__ B conv_to(double a) { return (B)a; }
+template <typename B> __device__ __forceinline__ B conv_to(float a) { return (B)a; }
+template <typename B> __device__ __forceinline__ B conv_to(double2 a);
+template <typename B> __device__ __forceinline__ B conv_to(float2 a);
+template <> __device__ __forceinline__ float2 conv_to<float2>(double2 a) { return make_float2((float)a.x, (float)a.y); }
+template <> __device__ __forceinline__ double2 conv_to<double2>(float2 a) { return make_double2(a.x, a.y); }
+template <typename A, typename B>
+__global__ void k_cast(const A* __restrict__ x, B* __restrict__ y, long long n) {
+  K_LOOP(n, i) y[i] = conv_to<B>(x[i]);
+}
+// y += x   (x in the other precision)
+template <typename A, typename B>
+__global__ void k_add_cast(const A* __restrict__ x, B* __restrict__ y, long long n) {
+  K_LOOP(n, i) y[i] = y[i] + conv_to<B>(x[i]);
+}
+// r = b - y
+template <typename T>
+__global__ void k_sub(const T* __restrict__ b, const T* __restrict__ y, T* __restrict__ r, long long n) {
+  K_LOOP(n, i) r[i] = b[i] - y[i];
+}
+
+template <typename T> class Solver;
+
 template <typename T>
 class Solver : public SolverBase {
  public:
@@ -200,6 +226,13 @@ class Solver : public SolverBase {
   size_t stage_bytes = 0;
   double cur_a = 1, cur_b = -1, cur_c = 0;
   Prof prof;
+  bool own_stream = true;
+  // run on another solver's stream (the mixed-precision psi helper)
+  void adopt_stream(cudaStream_t s2) {
+    VSAV_CUDA(cudaStreamSynchronize(st));
+    if (own_stream) VSAV_CUDA(cudaStreamDestroy(st));
+    st = s2; own_stream = false;
+  }
 
   template <typename X> X* dalloc(size_t n) {
     void* p = nullptr;
@@ -290,13 +323,29 @@ class Solver : public SolverBase {
     stage = dalloc<double>(nh);
     VSAV_CUDA(cudaStreamSynchronize(st));
     autotune();
+    if constexpr (std::is_same<T, double>::value) {
+      if (opt.psi_mixed && nd == 2) {
+        Options o2 = opt;
+        o2.psi_mixed = 0;
+        std::vector<int> rs(dm.R);
+        std::vector<double> pin(dm.V), pout(dm.V);
+        VSAV_CUDA(cudaMemcpy(pin.data(), d_psi_in, dm.V * sizeof(double), cudaMemcpyDeviceToHost));
+        VSAV_CUDA(cudaMemcpy(pout.data(), d_psi_out, dm.V * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int r = 0; r < dm.R; ++r) rs[r] = 0;
+        for (int v2 = 0; v2 < dm.V; ++v2) rs[run_of[v2]]++;
+        psi32 = new Solver<float>(dm, ph, o2, rs.data(), pin.data(), pout.data());
+        psi32->adopt_stream(st);
+      }
+    }
   }
 
   ~Solver() override {
     cudaStreamSynchronize(st);
+    if (psi32) { delete psi32; psi32 = nullptr; }
+    if (own_stream == false) st = nullptr;
     for (void* p : allocs) cudaFree(p);
     if (h_pinned_any) cudaFreeHost(h_pinned_any);
-    cudaStreamDestroy(st);
+    if (own_stream) cudaStreamDestroy(st);
   }
 
   bool psi_full() const { return opt.psi_form == 0; }
@@ -801,7 +850,7 @@ class Solver : public SolverBase {
 
   // y = P^-1 A in (+ dots), chunk by chunk: y-inverse (2 multipliers), fused
   // x pass (inverse, x M_psi, forward), y-forward, combine
-  void matvec(const C* in, C* out, int mode, const C* svec) {
+  void matvec(const C* in, C* out, int mode, const C* svec, bool precond = true) {
     const int V = dm.V;
     const long long F = 3LL * V, n = psi_n();
     const bool full = psi_full();
@@ -810,7 +859,7 @@ class Solver : public SolverBase {
     EW e = ew(n);
     VGeom vg{full ? 1 : 0, g.Nx, g.Ny, g.kp, g.nkx, ilog2(g.Nx), n, g.kxs, g.kys};
     SysMap sm{V, dm.R, d_run_of};
-    const double* pre = (opt.psi_precond >= 0) ? mmax_r : nullptr;
+    const double* pre = precond ? mmax_r : nullptr;
     for (int f0 = 0; f0 < F; f0 += Fc) {
       const int fc = (int)std::min<long long>(Fc, F - f0);
       C* t1 = vt12;
@@ -827,28 +876,47 @@ class Solver : public SolverBase {
     }
   }
 
-  void psi_solve() {
-    const int V = dm.V, R = dm.R, S = 3 * R;
-    const long long F = 3LL * V, VH = (long long)V * g.H, n = psi_n();
-    const bool full = psi_full();
-    // b = fft(irfft(rhs)) (FULL) / rfft(irfft(rhs)) (HALF)   (Solvers.jl:70-71)
+  // b = fft(irfft(rhs)) (FULL) / rfft(irfft(rhs)) (HALF)   (Solvers.jl:70-71)
+  void psi_prepare_b() {
+    const long long F = 3LL * dm.V;
     irfft(rhs, F, tmpP);
-    if (full) {
+    if (psi_full()) {
       rows_c2c<false>(nullptr, tmpP, vb, 1.0, F * g.Ny);
       cols(false, 3, F, vb, nullptr, 1, 0, M_ONE, 1, vb, 1);
     } else {
       rfft(tmpP, F, vb);
     }
-    C* x = full ? vx : cache + 5 * VH;
+  }
+  C* psi_x() { return psi_full() ? vx : cache + 5LL * dm.V * g.H; }
+  void psi_finish() {
+    const long long F = 3LL * dm.V, VH = (long long)dm.V * g.H;
+    if (psi_full()) { k_trunc<T><<<gridfor(F * g.Ny * g.kp), 256, 0, st>>>(vx, cache + 5 * VH, g.Nx, g.Ny, g.kp, g.nkx, (int)F); VSAV_COUNT_LAUNCH(); VSAV_LAUNCH_CHECK(); }
+  }
+  void psi_solve() {
+    if (opt.psi_mixed) { psi_solve_mixed(); return; }
+    psi_prepare_b();
+    psi_krylov(psi_x(), opt.psi_rtol, opt.psi_itmax);
+    psi_finish();
+  }
+
+  // ---- mixed precision: FP32 BiCGSTAB on FP64 residuals (iterative refinement)
+  Solver<float>* psi32 = nullptr;
+  void psi_solve_mixed();
+
+  // BiCGSTAB (Krylov.jl semantics) on b = vb from x0 = 0, result in x
+  void psi_krylov(C* x, double rtol, int itmax) {
+    const int V = dm.V, R = dm.R, S = 3 * R;
+    const long long F = 3LL * V, n = psi_n();
+    const bool full = psi_full();
     EW e = ew(n);
     VGeom vg{full ? 1 : 0, g.Nx, g.Ny, g.kp, g.nkx, ilog2(g.Nx), n, g.kxs, g.kys};
     SysMap sm{V, R, d_run_of};
     k_psi_init<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(vb, x, vr, vp, d_adt, mmax_r, ph.S4, vg, sm, e, part); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     fin(4, (int)F, e, fd);
-    k_bi_init<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, bupd, sm, S, (int)F, opt.psi_atol, opt.psi_rtol, opt.psi_itmax); VSAV_COUNT_LAUNCH();
+    k_bi_init<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, bupd, sm, S, (int)F, opt.psi_atol, rtol, itmax); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
-    for (int it = 0; it < opt.psi_itmax; ++it) {
+    for (int it = 0; it < itmax; ++it) {
       matvec(vp, vv, 0, nullptr);                       // v = M^-1 A p ; <c, v>
       fin(4, (int)F, e, fd);
       k_bi_alpha<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, sm, S, (int)F); VSAV_COUNT_LAUNCH();
@@ -861,7 +929,7 @@ class Solver : public SolverBase {
       VSAV_LAUNCH_CHECK();
       fin(4, (int)F, e, fd);
       VSAV_CUDA(cudaMemsetAsync(d_any, 0, sizeof(int), st));
-      k_bi_beta<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, bupd, sm, S, (int)F, opt.psi_itmax, d_any); VSAV_COUNT_LAUNCH();
+      k_bi_beta<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, bupd, sm, S, (int)F, itmax, d_any); VSAV_COUNT_LAUNCH();
       k_psi_p<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(vp, vr, vv, bst, bupd, sm, e); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
       if (opt.check_every_iter) {
@@ -872,7 +940,7 @@ class Solver : public SolverBase {
       // refresh the activity flags for the operator kernels of the next iteration
       k_bi_flags<<<(S + 63) / 64, 64, 0, st>>>(bst, bupd, S); VSAV_COUNT_LAUNCH();
     }
-    if (full) { k_trunc<T><<<gridfor(F * g.Ny * g.kp), 256, 0, st>>>(vx, cache + 5 * VH, g.Nx, g.Ny, g.kp, g.nkx, (int)F); VSAV_COUNT_LAUNCH(); VSAV_LAUNCH_CHECK(); }
+    (void)full;
   }
 
   // ------------------------------------------------------------------ host transfer
@@ -1032,5 +1100,42 @@ class Solver : public SolverBase {
   }
   cudaStream_t stream() override { return st; }
 };
+
+// Mixed precision (FP64 fields): b (FP64, full spectrum) -> x by sweeps of
+//   r = b - A x (FP64 operator, no preconditioner);  A d = r solved by the
+//   FP32 helper's BiCGSTAB to psi_inner_rtol;  x += d.
+// The FP32 solve does most of the work; the FP64 residual keeps the result at
+// FP64 accuracy after a few sweeps (classical iterative refinement).
+template <typename T>
+void Solver<T>::psi_solve_mixed() {
+  if constexpr (std::is_same<T, double>::value) {
+    Solver<float>* H = psi32;
+    const int V = dm.V, R = dm.R;
+    const long long F = 3LL * V, n = psi_n(), VP = (long long)V * g.P;
+    const long long nc = F * n;
+    k_cast<double, float><<<gridfor(VP), 256, 0, st>>>(Mpsi, H->Mpsi, VP); VSAV_COUNT_LAUNCH();
+    VSAV_CUDA(cudaMemcpyAsync(H->mmax_r, mmax_r, R * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    VSAV_CUDA(cudaMemcpyAsync(H->d_adt, d_adt, R * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    psi_prepare_b();
+    C* x = psi_x();
+    VSAV_CUDA(cudaMemsetAsync(x, 0, nc * sizeof(C), st));
+    VSAV_CUDA(cudaMemsetAsync(bupd, 0xff, 3 * R * sizeof(int), st));     // every system active in A x
+    for (int ref = 0; ref < std::max(1, opt.psi_refine); ++ref) {
+      const C* r = vb;
+      if (ref > 0) {
+        VSAV_CUDA(cudaMemsetAsync(bupd, 0xff, 3 * R * sizeof(int), st));
+        matvec(x, vt, 0, nullptr, false);
+        k_sub<C><<<gridfor(nc), 256, 0, st>>>(vb, vt, vs, nc); VSAV_COUNT_LAUNCH();
+        r = vs;
+      }
+      k_cast<double2, float2><<<gridfor(nc), 256, 0, st>>>(r, H->vb, nc); VSAV_COUNT_LAUNCH();
+      H->psi_krylov(H->psi_x(), opt.psi_inner_rtol, opt.psi_itmax);
+      k_add_cast<float2, double2><<<gridfor(nc), 256, 0, st>>>(H->psi_x(), x, nc); VSAV_COUNT_LAUNCH();
+      VSAV_LAUNCH_CHECK();
+    }
+    VSAV_CUDA(cudaMemcpyAsync(bst, H->bst, 3 * R * sizeof(BiState), cudaMemcpyDeviceToDevice, st));
+    psi_finish();
+  }
+}
 
 }  // namespace vsav

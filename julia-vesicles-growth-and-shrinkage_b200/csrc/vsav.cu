@@ -119,6 +119,9 @@ int vsav_create(const vsav_config* cfg, const vsav_options* opt, vsav_handle** o
     Options so;
     so.precision = o.precision; so.psi_form = o.psi_form; so.psi_precond = o.psi_precond;
     so.psi_itmax = o.psi_itmax; so.psi_rtol = o.psi_rtol; so.psi_atol = o.psi_atol;
+    if (o.precision != VSAV_FP64 && o.precision != VSAV_FP32 && o.precision != VSAV_MIXED)
+      throw std::runtime_error("precision must be VSAV_FP64, VSAV_FP32 or VSAV_MIXED");
+    so.psi_mixed = (o.precision == VSAV_MIXED && cfg->ndim == 2) ? 1 : 0;
     if (o.precision == VSAV_FP32)
       h->s = new Solver<float>(d, p, so, rs.data(), cfg->psi_in_v, cfg->psi_out_v);
     else

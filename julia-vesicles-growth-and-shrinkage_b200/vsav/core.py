@@ -26,7 +26,7 @@ class NotConvergedWarning(UserWarning):
     """psi BiCGSTAB hit itmax (the reference's @warn, Solvers.jl:76)."""
 
 
-PRECISION = {"fp64": 0, "fp32": 1}
+PRECISION = {"fp64": 0, "fp32": 1, "mixed": 2}
 PSI_FORM = {"full": 0, "half": 1}
 
 

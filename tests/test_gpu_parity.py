@@ -285,3 +285,18 @@ def test_steps_are_deterministic(prec):
         h.close()
     for a, b in zip(out[0], out[1]):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("name", ["single2d_n64", "multi2d_n64_N2"])
+def test_mixed_precision_vs_golden(name):
+    """FP64 fields with the psi BiCGSTAB in FP32 + FP64 iterative refinement:
+    FP64-level agreement with the oracle."""
+    kw, g = load_golden(name)
+    h = make(kw, precision="mixed")
+    h.init_state(g["phi0"], g["psi0"])
+    E, A = h.run(1, int(g["steps"]), monitor=True)
+    for k in FIELDS:
+        assert rel(h.get_field(k), g[k]) < 1e-9, (k, rel(h.get_field(k), g[k]))
+    np.testing.assert_allclose(h.get_scalars()[0], g["scalars"], rtol=1e-9)
+    np.testing.assert_allclose(E[:, 0], g["energy"], rtol=1e-9)
+    h.close()
