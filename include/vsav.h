@@ -60,7 +60,9 @@ typedef struct vsav_config {
 typedef struct vsav_options {
   int32_t precision;            /* VSAV_FP64 | VSAV_FP32 */
   int32_t psi_form;             /* VSAV_PSI_FULL | VSAV_PSI_HALF */
-  int32_t psi_precond;          /* 0 = diagonal spectral (Solvers.jl:57) */
+  int32_t psi_precond;          /* 0 = diagonal spectral on the left, Krylov.jl form (Solvers.jl:57,73-75);
+                                   1 = flexible right-preconditioned BiCGSTAB, diagonal;
+                                   2 = flexible, diagonal + learned correction (vsav_set_psi_net) */
   int32_t psi_itmax;            /* Solvers.jl:75 uses 20 */
   double psi_rtol;              /* Solvers.jl:75 uses conf.tol */
   double psi_atol;              /* Solvers.jl:74 uses 1e-14 */
@@ -136,7 +138,8 @@ int vsav_time_run(vsav_handle* h, int32_t n0, int32_t nsteps, const double* dt, 
  * the algorithmic bytes of the launch: inputs read once, outputs written once).
  * enable: 1 on, 0 off, 2 reset counters.  kclass: 0 FFT column pass, 1 x-pass
  * r2c, 2 x-pass c2r, 3 x-pass c2c, 4 fused psi x-pass (inverse, x M_psi,
- * forward), 5 psi operator combine.  out3 = (launches, total ms, total bytes). */
+ * forward), 5 psi operator combine, 6 pointwise, 7 learned-preconditioner network.
+ * out3 = (launches, total ms, total bytes). */
 int vsav_profile(vsav_handle* h, int32_t enable);
 /* kernels launched by this library so far (all handles) */
 int64_t vsav_launch_count(void);
@@ -158,6 +161,61 @@ int vsav_get_scalar_work(vsav_handle* h, int32_t what, double* out);
  * kind 0 rfft, 1 irfft, 10+m irfft of multiplier m * input
  * (m: 1 D1x, 2 D1y, 3 D1z, 4 Laplacian, 5 Biharmonic).  nf <= 3 V. */
 int vsav_transform(vsav_handle* h, int32_t kind, int32_t nf, const double* in, double* out);
+
+/* ---- learned psi preconditioner (no counterpart in the reference, whose
+ * Step-1 psi solve uses the diagonal spectral preconditioner only,
+ * Solvers.jl:53-75).  A network of five 3x3 convolutions, 2 -> 16 -> 16 -> 16
+ * -> 16 -> 1 channels with ReLU after the first four; parameters theta[7409]
+ * layer by layer W[o][i][ky][kx] then b[o]; convolution weights used
+ * BF16-rounded (nearest even), biases FP32, FP32 accumulation.  Inputs
+ * [B][2][H][W] float32, outputs [B][1][H'][W'] float32; periodic convolutions
+ * keep the size, valid ones shrink it by 10 (5 layers).  Host or device
+ * pointers are accepted. */
+typedef struct vsav_net vsav_net;
+/* cap_pixels: largest B*H*W of an input batch */
+int vsav_net_create(int64_t cap_pixels, int32_t device, vsav_net** out);
+int vsav_net_destroy(vsav_net* net);
+/* error text of the last failed call (net NULL: of the last failed vsav_net_create) */
+const char* vsav_net_last_error(const vsav_net* net);
+int vsav_net_nparams(void);
+/* sets the FP32 master parameters and resets the Adam state */
+int vsav_net_set_params(vsav_net* net, const double* theta);
+/* rounded != 0: the weights as used (BF16-rounded) */
+int vsav_net_get_params(vsav_net* net, double* theta, int32_t rounded);
+/* impl 0: FP32 per-layer kernels (periodic or valid); impl 1: the fused
+ * tensor-core kernel of the preconditioner (periodic; H, W powers of two,
+ * multiples of 32; BF16 activations) */
+int vsav_net_forward(vsav_net* net, const float* x, int32_t B, int32_t H, int32_t W, int32_t periodic,
+                     int32_t impl, float* out);
+/* loss = 1/2 sum (out - t)^2 and dloss/dtheta (host [7409]), FP32 kernels */
+int vsav_net_grad(vsav_net* net, const float* x, const float* t, int32_t B, int32_t H, int32_t W,
+                  int32_t periodic, double* loss, double* grad);
+/* nsteps Adam steps (betas 0.9/0.999, eps 1e-8, learning rate lr) on
+ * minibatches of `batch` crops drawn with replacement (seeded) from the crop
+ * sets x [ncrops][2][S][S] and t [ncrops][1][S-10][S-10] (device pointers,
+ * valid convolutions), minimising sum (out - t)^2 / sum t^2 of the batch;
+ * that loss per step is written to losses[nsteps] (host, may be NULL). */
+int vsav_net_train(vsav_net* net, const float* x, const float* t, int64_t ncrops, int32_t S, int32_t batch,
+                   int32_t nsteps, double lr, uint64_t seed, double* losses);
+/* sum (out - t)^2 / sum t^2 over a whole crop set, in chunks of `batch` */
+int vsav_net_eval(vsav_net* net, const float* x, const float* t, int64_t ncrops, int32_t S, int32_t batch,
+                  double* loss);
+
+/* Network parameters (theta[7409], layout above) of the learned psi
+ * preconditioner of a handle created with psi_precond = 2 (precision FP32 or
+ * MIXED, FULL psi form, 2D, Nx and Ny >= 32).  Must be set before the first
+ * Step 1.  (No counterpart in the reference.) */
+int vsav_set_psi_net(vsav_handle* h, const double* theta);
+/* Training-data harvest (no counterpart in the reference): with
+ * max_snapshots > 0 every later psi solve of the handle (FP64, FULL,
+ * psi_precond 0) keeps, in device memory, the physical real parts (FP32) of
+ * its BiCGSTAB iterates x_k and preconditioned residuals M^-1 (b - A x_k) for
+ * k = 0..max_snapshots-1, its final solution and M_psi; 0 turns it off.
+ * vsav_psi_harvest_read copies those of the last solve to out (host or device):
+ * [nsnap][2][3V][Ny][Nx] (x_k, r_k), then x* [3V][Ny][Nx], then M_psi
+ * [V][Ny][Nx]; out == NULL only reports nsnap and the float count needed. */
+int vsav_psi_harvest(vsav_handle* h, int32_t max_snapshots);
+int vsav_psi_harvest_read(vsav_handle* h, float* out, int64_t capacity, int32_t* nsnap, int64_t* nfloats);
 
 /* No counterpart in the reference (an addition of this library).
  * Inverse 2D real FFT in FP32 that allocates nothing, for callers that cannot

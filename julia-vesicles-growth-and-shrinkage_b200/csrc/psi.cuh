@@ -261,11 +261,14 @@ __global__ void k_psi_s(const cplx<T>* __restrict__ r, const cplx<T>* __restrict
 }
 
 // x = (x + alpha p) + omega s ;  r = s - omega t ; dots <c, r>, ||r||^2
+// (flexible right-preconditioned form: p and shat are the preconditioned
+// directions used for x, s the unpreconditioned one used for r)
 template <typename T>
 __global__ void __launch_bounds__(256) k_psi_update(cplx<T>* __restrict__ x, cplx<T>* __restrict__ r, const cplx<T>* __restrict__ p,
                                                     const cplx<T>* __restrict__ s, const cplx<T>* __restrict__ t,
                                                     const cplx<T>* __restrict__ cvec, const BiState* __restrict__ st,
-                                                    VGeom g, SysMap sm, EW ew, double2* part) {
+                                                    VGeom g, SysMap sm, EW ew, double2* part,
+                                                    const cplx<T>* __restrict__ shat = nullptr) {
   __shared__ double smm[2 * 4 * 8];
   KSum acc[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
   const int f = blockIdx.y;
@@ -279,12 +282,13 @@ __global__ void __launch_bounds__(256) k_psi_update(cplx<T>* __restrict__ x, cpl
       if (w == 0.0) continue;
       long long j = (long long)f * g.n + q;
       cplx<T> xv = x[j], pv = p[j], sv = s[j], tv = t[j];
+      const cplx<T> hv = shat ? shat[j] : sv;
       cplx<T> xa;
       xa.x = (double)xv.x + (al.x * (double)pv.x - al.y * (double)pv.y);
       xa.y = (double)xv.y + (al.x * (double)pv.y + al.y * (double)pv.x);
       cplx<T> xn;
-      xn.x = (double)xa.x + (om.x * (double)sv.x - om.y * (double)sv.y);
-      xn.y = (double)xa.y + (om.x * (double)sv.y + om.y * (double)sv.x);
+      xn.x = (double)xa.x + (om.x * (double)hv.x - om.y * (double)hv.y);
+      xn.y = (double)xa.y + (om.x * (double)hv.y + om.y * (double)hv.x);
       x[j] = xn;
       cplx<T> rn;
       rn.x = (double)sv.x - (om.x * (double)tv.x - om.y * (double)tv.y);
@@ -394,6 +398,60 @@ __global__ void k_bi_beta(const double* __restrict__ fd, BiState* __restrict__ s
   b.status = solved ? 1 : (brk ? 3 : (tired ? 2 : 0));
   st[sy] = b;
   if (b.active) atomicOr(any_active, 1);
+}
+
+// ---------------------------------------------------------------------------
+// flexible BiCGSTAB preconditioners (an addition: the reference preconditions
+// on the left with the diagonal only)
+// ---------------------------------------------------------------------------
+// out = D^-1 in,  D = a_dt + M_max S4 |k|^2  (the diagonal of Solvers.jl:57)
+template <typename T>
+__global__ void k_psi_diag(const cplx<T>* __restrict__ in, cplx<T>* __restrict__ out, const double* __restrict__ adt_r,
+                           const double* __restrict__ mmax_r, double S4, VGeom g, SysMap sm, EW ew) {
+  const int f = blockIdx.y;
+  const int r = sm.run_of[f % sm.V];
+  const double adt = adt_r[r], mm = mmax_r[r];
+  const long long beg = (long long)blockIdx.x * ew.chunk, end = min(ew.n, beg + ew.chunk);
+  for (long long q = beg + threadIdx.x; q < end; q += blockDim.x) {
+    int kx, ky; double kxv, kyv, w;
+    vk(g, q, kx, ky, kxv, kyv, w);
+    const long long j = (long long)f * g.n + q;
+    cplx<T> o{};
+    if (w != 0.0) {
+      double kxp = (!g.full && kx == g.Nx / 2) ? 0.0 : kxv;
+      double pinv = 1.0 / (adt + mm * S4 * (kxp * kxp + kyv * kyv));
+      cplx<T> v = in[j];
+      o.x = (double)v.x * pinv; o.y = (double)v.y * pinv;
+    }
+    out[j] = o;
+  }
+}
+
+// per-field sum of (Re w)^2 over a complex physical field [F][n]
+template <typename T>
+__global__ void __launch_bounds__(256) k_re_sumsq(const cplx<T>* __restrict__ w, EW ew, double2* part) {
+  __shared__ double smm[2 * 1 * 8];
+  KSum acc[1] = {{0, 0}};
+  const int f = blockIdx.y;
+  const long long beg = (long long)blockIdx.x * ew.chunk, end = min(ew.n, beg + ew.chunk);
+  for (long long q = beg + threadIdx.x; q < end; q += blockDim.x) {
+    const double v = (double)w[(long long)f * ew.n + q].x;
+    acc[0].add(v * v);
+  }
+  block_reduce_store<1>(acc, part + ((long long)f * ew.bpf + blockIdx.x), smm);
+}
+// inv_s[f] = 1 / RMS (0 for a zero field)
+__global__ void k_inv_rms(const double* __restrict__ fd, double n, float* __restrict__ inv_s, int F) {
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= F) return;
+  double ms = fd[f] / n;
+  inv_s[f] = ms > 0.0 ? (float)(1.0 / sqrt(ms)) : 0.f;
+}
+// out[i] = (float) Re z[i]
+template <typename T>
+__global__ void k_take_re(const cplx<T>* __restrict__ z, float* __restrict__ out, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = (float)z[i].x;
 }
 
 // full -> half truncation of the solution (Solvers.jl:79):  half[f][y][kx] = full[f][y][kx], kx < nkx

@@ -14,6 +14,7 @@
 #include <map>
 #include <mutex>
 #include "psi.cuh"
+#include "net_apply.cuh"
 
 namespace vsav {
 
@@ -22,7 +23,8 @@ enum FieldId : int { F_PHI = 0, F_PHI_HAT, F_PSI, F_PSI_HAT, F_U, F_U_HAT, F_P, 
 struct Options {
   int precision = 0;       // 0 FP64, 1 FP32 bulk
   int psi_form = 0;        // 0 FULL (reference form), 1 HALF
-  int psi_precond = 0;     // 0 diagonal, 1 learned (flexible)
+  int psi_precond = 0;     // 0 diagonal on the left (Krylov.jl form), 1 flexible right-preconditioned
+                          // BiCGSTAB with the diagonal, 2 the same with diagonal + learned correction
   int psi_itmax = 20;
   double psi_rtol = 1e-12, psi_atol = 1e-14;
   int check_every_iter = 1;  // read back convergence flags each BiCGSTAB iteration
@@ -68,6 +70,11 @@ class SolverBase {
   virtual void profile(int enable) = 0;
   virtual void profile_read(int cls, double* out3) = 0;
   virtual cudaStream_t stream() = 0;
+  // learned psi preconditioner: packed mma fragments + biases (net_pack)
+  virtual void set_psi_net(const uint32_t* frags, const float* bias) = 0;
+  // snapshots of the psi BiCGSTAB iterates (training data of the network)
+  virtual void harvest(int cap) = 0;
+  virtual long long harvest_read(float* out, long long cap, int* nsnap) = 0;
 };
 
 struct Dims {
@@ -131,7 +138,7 @@ __global__ void k_import_hat(const double* src, cplx<T>* dst, int Fo, int Fi, lo
 // handle's stream, plus the algorithmic bytes of each launch (inputs read once
 // + outputs written once).  Off unless enabled.
 // ---------------------------------------------------------------------------
-enum KClass : int { KC_COLS = 0, KC_ROWS_R2C, KC_ROWS_C2R, KC_ROWS_C2C, KC_ROWS_MUL, KC_PSI_VEC, KC_POINTWISE, KC_N };
+enum KClass : int { KC_COLS = 0, KC_ROWS_R2C, KC_ROWS_C2R, KC_ROWS_C2C, KC_ROWS_MUL, KC_PSI_VEC, KC_POINTWISE, KC_NET, KC_N };
 
 struct Prof {
   bool on = false;
@@ -219,6 +226,12 @@ class Solver : public SolverBase {
   int* d_err;
   // psi solver
   C *vb, *vx, *vr, *vp, *vv, *vs, *vt, *vt12;
+  C *vph = nullptr, *vsh = nullptr;          // preconditioned directions (flexible BiCGSTAB)
+  uint32_t* nfrag = nullptr;                 // learned preconditioner weights (mma fragments)
+  float *nbias = nullptr, *inv_s = nullptr;
+  bool net_ok = false;
+  float* hv = nullptr;                       // harvested iterates
+  int hv_cap = 0, hv_count = 0;
   BiState* bst; int *bupd, *d_any;
   int* h_pinned_any = nullptr;
   StepStatus last;
@@ -317,6 +330,18 @@ class Solver : public SolverBase {
       vx = psi_full() ? dalloc<C>(3 * V * n) : nullptr;
       bst = dalloc<BiState>(3 * R); bupd = dalloc<int>(3 * R); d_any = dalloc<int>(1);
       VSAV_CUDA(cudaMallocHost(&h_pinned_any, sizeof(int)));
+      if (opt.psi_precond < 0 || opt.psi_precond > 2) throw std::runtime_error("psi_precond must be 0, 1 or 2");
+      if (opt.psi_precond >= 1 && !opt.psi_mixed) {
+        vph = dalloc<C>(3 * V * n); vsh = dalloc<C>(3 * V * n);
+      }
+      if (opt.psi_precond == 2 && !opt.psi_mixed) {
+        if (!std::is_same<T, float>::value)
+          throw std::runtime_error("the learned psi preconditioner runs in the FP32 psi solve (precision fp32 or mixed)");
+        if (!psi_full()) throw std::runtime_error("the learned psi preconditioner needs the full-spectrum psi form");
+        if (g.Nx < NA_T || g.Ny < NA_T) throw std::runtime_error("the learned psi preconditioner needs Nx, Ny >= 32");
+        nfrag = dalloc<uint32_t>(NF_WORDS); nbias = dalloc<float>(NF_BIAS); inv_s = dalloc<float>(3 * V);
+        VSAV_CUDA(cudaFuncSetAttribute(k_net_apply<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, NA_SMEM));
+      }
     }
     long long nh = std::max<long long>(3LL * V, 2LL * R * nd) * std::max<long long>(g.P, (long long)g.Nz * g.Ny * g.nkx * 2);
     stage_bytes = nh * sizeof(double);
@@ -341,6 +366,7 @@ class Solver : public SolverBase {
 
   ~Solver() override {
     cudaStreamSynchronize(st);
+    if (hv) cudaFree(hv);
     if (psi32) { delete psi32; psi32 = nullptr; }
     if (own_stream == false) st = nullptr;
     for (void* p : allocs) cudaFree(p);
@@ -410,7 +436,7 @@ class Solver : public SolverBase {
       size_t sm = rows_smem(L, nl);
       set_smem_attr<E_, NT_>((const void*)k_rows_r2c<T, E_, NT_>, sm);
       prof.begin(st);
-      k_rows_r2c<T, E_, NT_><<<(unsigned)grid, thr, sm, st>>>(in0, in1, (T)a0, (T)a1, out, logL, lognl, nrows, g.kp, tab);
+      k_rows_r2c<T, E_, NT_><<<(unsigned)grid, thr, sm, st>>>(in0, in1, (T)a0, (T)a1, out, logL, lognl, nrows, g.kp, tab); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
       prof.end(st, KC_ROWS_R2C, (double)nrows * (g.Nx * sizeof(T) * (in1 ? 2 : 1) + g.nkx * sizeof(C)));
     })
@@ -425,7 +451,7 @@ class Solver : public SolverBase {
       size_t sm = rows_smem(L, nl);
       set_smem_attr<E_, NT_>((const void*)k_rows_c2r<T, E_, NT_>, sm);
       prof.begin(st);
-      k_rows_c2r<T, E_, NT_><<<(unsigned)grid, thr, sm, st>>>(in, out, (T)scale, logL, lognl, nrows, g.kp, tab);
+      k_rows_c2r<T, E_, NT_><<<(unsigned)grid, thr, sm, st>>>(in, out, (T)scale, logL, lognl, nrows, g.kp, tab); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
       prof.end(st, KC_ROWS_C2R, (double)nrows * (g.Nx * sizeof(T) + g.nkx * sizeof(C)));
     })
@@ -441,7 +467,7 @@ class Solver : public SolverBase {
       size_t sm = rows_smem(L, nl);
       set_smem_attr<E_, NT_>((const void*)k_rows_c2c<T, E_, NT_, INV>, sm);
       prof.begin(st);
-      k_rows_c2c<T, E_, NT_, INV><<<(unsigned)grid, thr, sm, st>>>(in, in_real, out, (T)scale, logL, lognl, nrows, tab);
+      k_rows_c2c<T, E_, NT_, INV><<<(unsigned)grid, thr, sm, st>>>(in, in_real, out, (T)scale, logL, lognl, nrows, tab); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
       prof.end(st, KC_ROWS_C2C, (double)nrows * g.Nx * ((in_real ? sizeof(T) : sizeof(C)) + sizeof(C)));
     })
@@ -905,6 +931,7 @@ class Solver : public SolverBase {
 
   // BiCGSTAB (Krylov.jl semantics) on b = vb from x0 = 0, result in x
   void psi_krylov(C* x, double rtol, int itmax) {
+    if (opt.psi_precond >= 1) { psi_flex(x, rtol, itmax); return; }
     const int V = dm.V, R = dm.R, S = 3 * R;
     const long long F = 3LL * V, n = psi_n();
     const bool full = psi_full();
@@ -916,6 +943,7 @@ class Solver : public SolverBase {
     fin(4, (int)F, e, fd);
     k_bi_init<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, bupd, sm, S, (int)F, opt.psi_atol, rtol, itmax); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
+    if (hv_cap) { hv_count = 0; harvest_snap(x, vr); }
     for (int it = 0; it < itmax; ++it) {
       matvec(vp, vv, 0, nullptr);                       // v = M^-1 A p ; <c, v>
       fin(4, (int)F, e, fd);
@@ -932,6 +960,7 @@ class Solver : public SolverBase {
       k_bi_beta<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, bupd, sm, S, (int)F, itmax, d_any); VSAV_COUNT_LAUNCH();
       k_psi_p<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(vp, vr, vv, bst, bupd, sm, e); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
+      if (hv_cap && hv_count < hv_cap) harvest_snap(x, vr);
       if (opt.check_every_iter) {
         VSAV_CUDA(cudaMemcpyAsync(h_pinned_any, d_any, sizeof(int), cudaMemcpyDeviceToHost, st));
         VSAV_CUDA(cudaStreamSynchronize(st));
@@ -940,7 +969,149 @@ class Solver : public SolverBase {
       // refresh the activity flags for the operator kernels of the next iteration
       k_bi_flags<<<(S + 63) / 64, 64, 0, st>>>(bst, bupd, S); VSAV_COUNT_LAUNCH();
     }
+    if (hv_cap) harvest_final(x);
     (void)full;
+  }
+
+  // ---- flexible right-preconditioned BiCGSTAB (an addition; the reference
+  // solve is the left-preconditioned psi_krylov above).  x0 = 0, shadow c = b,
+  // stop on ||b - A x|| <= atol + rtol ||b|| or itmax.  The preconditioner P
+  // may change between applications (learned correction): x is built from the
+  // stored preconditioned directions p^ = P p, s^ = P s.
+  //   p^ = P p; v = A p^; alpha = rho / <c, v>; s = r - alpha v
+  //   s^ = P s; t = A s^; omega = <t, s> / <t, t>
+  //   x += alpha p^ + omega s^; r = s - omega t; beta = (rho'/rho)(alpha/omega)
+  //   p = r + beta (p - omega v)
+  VGeom vgeom() const {
+    return VGeom{psi_full() ? 1 : 0, g.Nx, g.Ny, g.kp, g.nkx, ilog2(g.Nx), psi_n(), g.kxs, g.kys};
+  }
+  void psi_flex(C* x, double rtol, int itmax) {
+    const int V = dm.V, R = dm.R, S = 3 * R;
+    const long long F = 3LL * V, n = psi_n();
+    EW e = ew(n);
+    VGeom vg = vgeom();
+    SysMap sm{V, R, d_run_of};
+    if (opt.psi_precond == 2 && !net_ok)
+      throw std::runtime_error("learned psi preconditioner selected but no network loaded (vsav_set_psi_net)");
+    k_psi_init<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(vb, x, vr, vp, d_adt, nullptr, ph.S4, vg, sm, e, part); VSAV_COUNT_LAUNCH();
+    VSAV_LAUNCH_CHECK();
+    fin(4, (int)F, e, fd);
+    k_bi_init<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, bupd, sm, S, (int)F, opt.psi_atol, rtol, itmax); VSAV_COUNT_LAUNCH();
+    VSAV_LAUNCH_CHECK();
+    for (int it = 0; it < itmax; ++it) {
+      precond_apply(vp, vph);
+      matvec(vph, vv, 0, nullptr, false);               // v = A p^ ; <c, v>
+      fin(4, (int)F, e, fd);
+      k_bi_alpha<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, sm, S, (int)F); VSAV_COUNT_LAUNCH();
+      k_psi_s<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(vr, vv, vs, bst, sm, e); VSAV_COUNT_LAUNCH();
+      VSAV_LAUNCH_CHECK();
+      precond_apply(vs, vsh);
+      matvec(vsh, vt, 1, vs, false);                    // t = A s^ ; <t, s>, <t, t>
+      fin(4, (int)F, e, fd);
+      k_bi_omega<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, sm, S, (int)F); VSAV_COUNT_LAUNCH();
+      k_psi_update<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(x, vr, vph, vs, vt, vb, bst, vg, sm, e, part, vsh); VSAV_COUNT_LAUNCH();
+      VSAV_LAUNCH_CHECK();
+      fin(4, (int)F, e, fd);
+      VSAV_CUDA(cudaMemsetAsync(d_any, 0, sizeof(int), st));
+      k_bi_beta<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, bupd, sm, S, (int)F, itmax, d_any); VSAV_COUNT_LAUNCH();
+      k_psi_p<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(vp, vr, vv, bst, bupd, sm, e); VSAV_COUNT_LAUNCH();
+      VSAV_LAUNCH_CHECK();
+      if (opt.check_every_iter) {
+        VSAV_CUDA(cudaMemcpyAsync(h_pinned_any, d_any, sizeof(int), cudaMemcpyDeviceToHost, st));
+        VSAV_CUDA(cudaStreamSynchronize(st));
+        if (!*h_pinned_any) break;
+      }
+      k_bi_flags<<<(S + 63) / 64, 64, 0, st>>>(bst, bupd, S); VSAV_COUNT_LAUNCH();
+    }
+  }
+
+  // full-spectrum inverse 2D FFT of F = 3V vectors (normalised), in -> out
+  void ifft_full(const C* in, C* out) {
+    const long long F = 3LL * dm.V;
+    cols(true, 3, F, in, nullptr, 1, 0, M_ONE, 1, out, 1);
+    rows_c2c<true>(out, nullptr, out, 1.0 / (double)g.P, F * g.Ny);
+  }
+
+  // out = P in.  Diagonal: D^-1 in.  Learned: D^-1 in + FFT(s * net(y / s, M~)),
+  // y = Re IFFT(D^-1 in) per field, s its RMS, M~ = (M_psi - 0.075) / 0.025.
+  void precond_apply(const C* in, C* out) {
+    const long long F = 3LL * dm.V, n = psi_n();
+    EW e = ew(n);
+    SysMap sm{dm.V, dm.R, d_run_of};
+    k_psi_diag<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(in, out, d_adt, mmax_r, ph.S4, vgeom(), sm, e); VSAV_COUNT_LAUNCH();
+    VSAV_LAUNCH_CHECK();
+    if (opt.psi_precond != 2) return;
+    if constexpr (std::is_same<T, float>::value) {
+      C* w1 = vt12;
+      C* w2 = vt12 + F * n;
+      ifft_full(out, w1);
+      k_re_sumsq<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(w1, e, part); VSAV_COUNT_LAUNCH();
+      VSAV_LAUNCH_CHECK();
+      fin(1, (int)F, e, fd2);
+      k_inv_rms<<<(unsigned)((F + 127) / 128), 128, 0, st>>>(fd2, (double)n, inv_s, (int)F); VSAV_COUNT_LAUNCH();
+      prof.begin(st);
+      k_net_apply<1><<<dim3((unsigned)((g.Ny / NA_T) * (g.Nx / NA_T)), (unsigned)F), NA_THREADS, NA_SMEM, st>>>(
+          w1, Mpsi, inv_s, w2, g.Ny, g.Nx, dm.V, nfrag, nbias); VSAV_COUNT_LAUNCH();
+      VSAV_LAUNCH_CHECK();
+      prof.end(st, KC_NET, (double)F * n * (2.0 * sizeof(C)) + (double)dm.V * g.P * sizeof(T));
+      rows_c2c<false>(w2, nullptr, w2, 1.0, F * g.Ny);
+      cols(false, 3, F, w2, nullptr, 1, 0, M_ONE, 1, out, 1);
+    }
+  }
+
+  void set_psi_net(const uint32_t* frags, const float* bias) override {
+    if (psi32) { psi32->set_psi_net(frags, bias); return; }
+    if (!nfrag) throw std::runtime_error("the handle was not created with the learned psi preconditioner (psi_precond = 2)");
+    VSAV_CUDA(cudaMemcpyAsync(nfrag, frags, NF_WORDS * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    VSAV_CUDA(cudaMemcpyAsync(nbias, bias, NF_BIAS * sizeof(float), cudaMemcpyHostToDevice, st));
+    VSAV_CUDA(cudaStreamSynchronize(st));
+    net_ok = true;
+  }
+
+  // ---- harvest of (x_k, r~_k) pairs of the reference-form BiCGSTAB: physical
+  // real parts (FP32) of every iterate of the last psi solve, the final
+  // solution and M_psi.  Layout: [cap][2][3V][P] | x* [3V][P] | M [V][P].
+  void harvest(int cap) override {
+    if (cap < 0) throw std::runtime_error("harvest capacity must be >= 0");
+    if (cap > 0 && (g.nd != 2 || !psi_full() || opt.psi_precond != 0 || opt.psi_mixed))
+      throw std::runtime_error("harvest needs a 2D handle with the reference-form psi solve (FULL, psi_precond 0, not mixed)");
+    if (hv) { VSAV_CUDA(cudaStreamSynchronize(st)); VSAV_CUDA(cudaFree(hv)); hv = nullptr; }
+    hv_cap = cap; hv_count = 0;
+    if (cap > 0) {
+      const long long FP = 3LL * dm.V * g.P;
+      VSAV_CUDA(cudaMalloc(&hv, ((2LL * cap + 1) * FP + (long long)dm.V * g.P) * sizeof(float)));
+    }
+  }
+  void harvest_snap(const C* x, const C* r) {
+    const long long FP = 3LL * dm.V * g.P;
+    float* dst = hv + (long long)hv_count * 2 * FP;
+    ifft_full(x, vt12);
+    k_take_re<T><<<gridfor(FP), 256, 0, st>>>(vt12, dst, FP); VSAV_COUNT_LAUNCH();
+    ifft_full(r, vt12);
+    k_take_re<T><<<gridfor(FP), 256, 0, st>>>(vt12, dst + FP, FP); VSAV_COUNT_LAUNCH();
+    VSAV_LAUNCH_CHECK();
+    ++hv_count;
+  }
+  void harvest_final(const C* x) {
+    const long long FP = 3LL * dm.V * g.P, VP = (long long)dm.V * g.P;
+    float* dst = hv + 2LL * hv_cap * FP;
+    ifft_full(x, vt12);
+    k_take_re<T><<<gridfor(FP), 256, 0, st>>>(vt12, dst, FP); VSAV_COUNT_LAUNCH();
+    k_cast<T, float><<<gridfor(VP), 256, 0, st>>>(Mpsi, dst + FP, VP); VSAV_COUNT_LAUNCH();
+    VSAV_LAUNCH_CHECK();
+  }
+  long long harvest_read(float* out, long long cap, int* nsnap) override {
+    if (!hv) throw std::runtime_error("harvest is not enabled");
+    const long long FP = 3LL * dm.V * g.P, VP = (long long)dm.V * g.P;
+    const long long need = 2LL * hv_count * FP + FP + VP;
+    if (nsnap) *nsnap = hv_count;
+    if (!out) return need;
+    if (cap < need) throw std::runtime_error("harvest output buffer too small: " + std::to_string(need) + " floats needed");
+    VSAV_CUDA(cudaMemcpyAsync(out, hv, 2LL * hv_count * FP * sizeof(float), cudaMemcpyDefault, st));
+    VSAV_CUDA(cudaMemcpyAsync(out + 2LL * hv_count * FP, hv + 2LL * hv_cap * FP, (FP + VP) * sizeof(float),
+                              cudaMemcpyDefault, st));
+    VSAV_CUDA(cudaStreamSynchronize(st));
+    return need;
   }
 
   // ------------------------------------------------------------------ host transfer
@@ -1087,8 +1258,10 @@ class Solver : public SolverBase {
     return s;
   }
   void sync() override { VSAV_CUDA(cudaStreamSynchronize(st)); }
+  // the FP32 psi helper of the mixed mode is profiled with its owner
   void profile(int enable) override {
     VSAV_CUDA(cudaStreamSynchronize(st));
+    if (psi32) psi32->profile(enable);
     if (enable == 2) { prof.reset(); return; }
     prof.collect();
     prof.enable(enable != 0);
@@ -1097,6 +1270,11 @@ class Solver : public SolverBase {
     VSAV_CUDA(cudaStreamSynchronize(st));
     prof.collect();
     out3[0] = (double)prof.launches[cls]; out3[1] = prof.ms[cls]; out3[2] = prof.bytes[cls];
+    if (psi32) {
+      double o[3];
+      psi32->profile_read(cls, o);
+      out3[0] += o[0]; out3[1] += o[1]; out3[2] += o[2];
+    }
   }
   cudaStream_t stream() override { return st; }
 };

@@ -294,4 +294,34 @@ int vsav_transform(vsav_handle* h, int32_t kind, int32_t nf, const double* in, d
   });
 }
 
+int vsav_set_psi_net(vsav_handle* h, const double* theta) {
+  return guard(h, [&] {
+    if (!theta) throw std::runtime_error("theta is NULL");
+    if (h->nd != 2) throw std::runtime_error("the learned psi preconditioner is 2D only");
+    std::vector<float> wb(NET_NPARAM);
+    for (int k = 0; k < NET_NPARAM; ++k) wb[k] = (float)theta[k];
+    for (int l = 0; l < NET_NL; ++l)
+      for (int k = net_woff(l); k < net_woff(l) + net_wsize(l); ++k) wb[k] = bf16_round(wb[k]);
+    std::vector<uint32_t> fr(NF_WORDS);
+    std::vector<float> bias(NF_BIAS, 0.f);
+    net_pack(wb.data(), fr.data(), bias.data());
+    h->s->set_psi_net(fr.data(), bias.data());
+    return VSAV_OK;
+  });
+}
+
+int vsav_psi_harvest(vsav_handle* h, int32_t max_snapshots) {
+  return guard(h, [&] { h->s->harvest(max_snapshots); return VSAV_OK; });
+}
+
+int vsav_psi_harvest_read(vsav_handle* h, float* out, int64_t capacity, int32_t* nsnap, int64_t* nfloats) {
+  return guard(h, [&] {
+    int ns = 0;
+    long long need = h->s->harvest_read(out, capacity, &ns);
+    if (nsnap) *nsnap = ns;
+    if (nfloats) *nfloats = need;
+    return VSAV_OK;
+  });
+}
+
 }  // extern "C"

@@ -24,6 +24,9 @@ EXPORTS = ("vsav_create", "vsav_destroy", "vsav_last_error", "vsav_create_error"
            "vsav_step4", "vsav_step5", "vsav_step6", "vsav_step7", "vsav_update_state", "vsav_run",
            "vsav_monitor", "vsav_get_work", "vsav_get_scalar_work", "vsav_transform", "vsav_time_run",
            "vsav_profile", "vsav_profile_read", "vsav_launch_count",
+           "vsav_net_create", "vsav_net_destroy", "vsav_net_last_error", "vsav_net_nparams",
+           "vsav_net_set_params", "vsav_net_get_params", "vsav_net_forward", "vsav_net_grad", "vsav_net_train",
+           "vsav_net_eval", "vsav_set_psi_net", "vsav_psi_harvest", "vsav_psi_harvest_read",
            "vsav_irfft2d_f32_noalloc", "vsav_noalloc_error")
 
 
@@ -102,6 +105,20 @@ def load(path: str = LIB_PATH):
         "vsav_irfft2d_f32_noalloc": ([ct.c_void_p, ct.c_void_p, i32, i32, i32, ct.c_double, ct.c_double, i32,
                                       ct.c_void_p], ct.c_int),
         "vsav_noalloc_error": ([], ct.c_char_p),
+        "vsav_net_create": ([ct.c_int64, i32, ct.POINTER(ct.c_void_p)], ct.c_int),
+        "vsav_net_destroy": ([H], ct.c_int),
+        "vsav_net_last_error": ([H], ct.c_char_p),
+        "vsav_net_nparams": ([], ct.c_int),
+        "vsav_net_set_params": ([H, D], ct.c_int),
+        "vsav_net_get_params": ([H, D, i32], ct.c_int),
+        "vsav_net_forward": ([H, ct.c_void_p, i32, i32, i32, i32, i32, ct.c_void_p], ct.c_int),
+        "vsav_net_grad": ([H, ct.c_void_p, ct.c_void_p, i32, i32, i32, i32, D, D], ct.c_int),
+        "vsav_net_train": ([H, ct.c_void_p, ct.c_void_p, ct.c_int64, i32, i32, i32, ct.c_double, ct.c_uint64, D],
+                           ct.c_int),
+        "vsav_net_eval": ([H, ct.c_void_p, ct.c_void_p, ct.c_int64, i32, i32, D], ct.c_int),
+        "vsav_set_psi_net": ([H, D], ct.c_int),
+        "vsav_psi_harvest": ([H, i32], ct.c_int),
+        "vsav_psi_harvest_read": ([H, ct.c_void_p, ct.c_int64, ct.POINTER(i32), ct.POINTER(ct.c_int64)], ct.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)

@@ -28,14 +28,21 @@ class NotConvergedWarning(UserWarning):
 
 PRECISION = {"fp64": 0, "fp32": 1, "mixed": 2}
 PSI_FORM = {"full": 0, "half": 1}
+PSI_PRECOND = {"diag": 0, "flex_diag": 1, "learned": 2}
 
 
 class Handle:
     def __init__(self, cfg, precision: str = "fp64", psi_form: Optional[str] = None,
                  run_sizes: Optional[Sequence[int]] = None, psi_itmax: int = 20,
-                 psi_rtol: Optional[float] = None, psi_atol: float = 1e-14, device: int = 0):
+                 psi_rtol: Optional[float] = None, psi_atol: float = 1e-14, device: int = 0,
+                 psi_precond: str = "diag", psi_net=None):
         """cfg: any object with the reference Config fields (Types.jl:27-74);
-        psi_in_v / psi_out_v hold one value per vesicle field of all runs."""
+        psi_in_v / psi_out_v hold one value per vesicle field of all runs.
+        psi_precond: "diag" (the reference's left-preconditioned BiCGSTAB),
+        "flex_diag" / "learned" (flexible right-preconditioned BiCGSTAB with the
+        diagonal, or the diagonal plus the learned correction whose parameters
+        psi_net gives: an array of 7409 values or a path to an .npz with
+        "theta")."""
         self.lib = L.load()
         self.nd = 3 if getattr(cfg, "Nz", 0) else 2
         self.Nx, self.Ny = int(cfg.Nx), int(cfg.Ny)
@@ -63,6 +70,8 @@ class Handle:
         self.lib.vsav_default_options(ct.byref(o), ct.byref(c))
         o.precision = PRECISION[precision]
         o.psi_form = PSI_FORM[self.psi_form]
+        o.psi_precond = PSI_PRECOND[psi_precond]
+        self.psi_precond = psi_precond
         o.psi_itmax = psi_itmax
         o.psi_rtol = cfg.tol if psi_rtol is None else psi_rtol
         o.psi_atol = psi_atol
@@ -76,6 +85,8 @@ class Handle:
             raise VsavError(rc, self.lib.vsav_create_error().decode())
         self.h = h
         self.last_status = L.VsavStatus()
+        if psi_net is not None:
+            self.set_psi_net(psi_net)
 
     # -- lifetime -----------------------------------------------------------
     def close(self):
@@ -207,7 +218,8 @@ class Handle:
         self._chk(self.lib.vsav_time_run(self.h, n0, nsteps, None, int(monitor), L.dptr(ms)))
         return float(ms[0])
 
-    KCLASS = ("fft_cols", "fft_rows_r2c", "fft_rows_c2r", "fft_rows_c2c", "psi_rows_fused", "psi_combine")
+    KCLASS = ("fft_cols", "fft_rows_r2c", "fft_rows_c2r", "fft_rows_c2c", "psi_rows_fused", "psi_combine",
+              "pointwise", "psi_net")
 
     def profile(self, enable):
         self._chk(self.lib.vsav_profile(self.h, {True: 1, False: 0, "reset": 2}[enable]))
@@ -276,3 +288,40 @@ class Handle:
         out = np.empty((nf,) + self.sp)
         self._chk(self.lib.vsav_transform(self.h, kind, nf, L.dptr(F), L.dptr(out)))
         return out.reshape(F.shape[:-self.nd] + self.sp)
+
+    # -- learned psi preconditioner ----------------------------------------
+    def set_psi_net(self, theta):
+        """Network parameters of the learned psi preconditioner (array of 7409
+        values or path of an .npz holding "theta")."""
+        if isinstance(theta, str):
+            theta = np.load(theta)["theta"]
+        th = np.ascontiguousarray(theta, dtype=np.float64)
+        if th.size != self.lib.vsav_net_nparams():
+            raise ValueError("theta must hold %d values" % self.lib.vsav_net_nparams())
+        self._chk(self.lib.vsav_set_psi_net(self.h, L.dptr(th)))
+
+    def harvest(self, max_snapshots: int):
+        """Keep the BiCGSTAB iterates of every later psi solve (0: off)."""
+        self._chk(self.lib.vsav_psi_harvest(self.h, int(max_snapshots)))
+
+    def harvest_read(self, out=None):
+        """Iterates of the last psi solve: (x [K][3V][Ny][Nx], r [K][3V][Ny][Nx],
+        x_star [3V][Ny][Nx], M [V][Ny][Nx]) as float32 arrays; physical real
+        parts, r = M^-1 (b - A x_k).  With `out` (a device buffer address and
+        its capacity in floats) the data is copied there instead and
+        (nsnap, nfloats) is returned."""
+        ns = ct.c_int32()
+        nf = ct.c_int64()
+        if out is not None:
+            ptr, cap = out
+            self._chk(self.lib.vsav_psi_harvest_read(self.h, ct.c_void_p(ptr), int(cap), ct.byref(ns), ct.byref(nf)))
+            return ns.value, nf.value
+        self._chk(self.lib.vsav_psi_harvest_read(self.h, None, 0, ct.byref(ns), ct.byref(nf)))
+        buf = np.empty(nf.value, np.float32)
+        self._chk(self.lib.vsav_psi_harvest_read(self.h, buf.ctypes.data_as(ct.c_void_p), buf.size, ct.byref(ns),
+                                                 ct.byref(nf)))
+        K, F, P = ns.value, 3 * self.V, self.Nx * self.Ny
+        xr = buf[:2 * K * F * P].reshape(K, 2, F, self.Ny, self.Nx)
+        xs = buf[2 * K * F * P:(2 * K + 1) * F * P].reshape(F, self.Ny, self.Nx)
+        M = buf[(2 * K + 1) * F * P:].reshape(self.V, self.Ny, self.Nx)
+        return xr[:, 0], xr[:, 1], xs, M
