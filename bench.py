@@ -6,12 +6,15 @@
 Workload (N=1): 2D, 1024^2 grid, 8 vesicles (seeded non-overlapping ellipses,
 radii U[0.4,0.7]), dt = 1e-6, one time step = Steps 1-7 of the reference
 (src/Solvers.jl) + state update + the per-step monitoring of
-src/simulation.jl:146-148 (modified energy, area ratio).  Our arm runs the mixed
-path: FP64 fields, FFTs and SAV scalars, with the psi BiCGSTAB (the dominant
-cost) in FP32 and refined against FP64 residuals, which keeps every field within
-1e-5 of FP64 (measured ~1e-10).  The same workload is timed on the plain FP64
-path (the "plain FP64 diagonal BiCGSTAB GPU solver") and on the FP32-bulk path,
-whose error is reported beside it.
+src/simulation.jl:146-148 (modified energy, area ratio).  The headline arm
+("learned") runs FP64 fields, FFTs and SAV scalars with the psi solve (the
+dominant cost) as a flexible BiCGSTAB in FP32, preconditioned by the diagonal
+plus the learned network correction, refined against FP64 residuals.  Beside
+it, on the same workload: the same solver with the diagonal alone
+("flex_diag"), the Krylov.jl-form inner solve ("mixed_krylov_diag"), the plain
+FP64 reference-form solver ("fp64_diag": the plain FP64 diagonal BiCGSTAB GPU
+solver) and the FP32-bulk path with the learned preconditioner, each with its
+relative L2 error against the FP64 solver after 3 steps.
 
 N>1 (torchrun): replicas only -- each rank advances its own seeded run, no
 data-path collective; value = all ranks' steps / max-over-ranks device time.
@@ -195,14 +198,30 @@ def run_reference(args):
 
 
 # --------------------------------------------------------------------- ours
+NET_FLOP_PER_PIXEL = 2 * (2 * 16 * 9 + 3 * 16 * 16 * 9 + 16 * 9)     # 14688: five 3x3 conv layers
+WEIGHTS = os.path.join(PKG, "vsav", "precond_weights.npz")
+# the configurations timed on the same workload (the headline is --arm)
+ARMS = {
+    "mixed_krylov_diag": dict(precision="mixed", psi_precond="diag"),
+    "learned": dict(precision="mixed", psi_precond="learned", psi_net=WEIGHTS),
+    "flex_diag": dict(precision="mixed", psi_precond="flex_diag"),
+    "fp64_diag": dict(precision="fp64", psi_precond="diag"),
+    "fp32_bulk_learned": dict(precision="fp32", psi_precond="learned", psi_net=WEIGHTS, psi_rtol=1e-6, psi_itmax=60),
+}
+
+
 def run_ours(args):
     ws, rank, local = dist_init()
     from vsav import Handle, _lib
     hbm, peak_kind = peaks()
+    try:
+        tflops_peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"])
+    except Exception:
+        tflops_peak = 1590.0
     kw, phi, psi = workload(rank)
     V = kw["N"]
-    MAIN = dict(precision="mixed", psi_form="full", device=local)
-    h = Handle(Cfg(**kw), **MAIN)
+    head = args.arm
+    h = Handle(Cfg(**kw), device=local, **ARMS[head])
     h.init_state(phi, psi)
     n = 1
     h.run(n, args.warmup, monitor=True)
@@ -222,7 +241,7 @@ def run_ours(args):
     if args.quick:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
-                              "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "quick": True,
+                              "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "quick": True, "arm": head,
                               "gpu_launches": int(launches), "clocks": clocks, "psi_iters_last_step": iters}), flush=True)
         h.close()
         return
@@ -269,40 +288,43 @@ def run_ours(args):
     h.profile(False)
     prof = h.profile_read()
     h.profile("reset")
-    dom = max(prof, key=lambda k: prof[k]["ms"])
+    h.close()
+    byte_classes = {k: v for k, v in prof.items() if k != "psi_net"}
+    dom = max(byte_classes, key=lambda k: byte_classes[k]["ms"])
     d = prof[dom]
     per_launch_bytes = d["bytes"] / max(d["launches"], 1)
     per_launch_ms = d["ms"] / max(d["launches"], 1)
     achieved = per_launch_bytes / (per_launch_ms / 1000.0) / 1e9 if per_launch_ms > 0 else 0.0
-    traffic = None
+    # DRAM bytes of one ncu-captured launch of the class (profiles/traffic.json),
+    # scaled by algorithmic bytes to this class's average launch
+    traffic, traffic_note = None, None
     tr_path = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tr_path):
         try:
-            traffic = json.load(open(tr_path)).get(dom)
+            tr = json.load(open(tr_path)).get(dom)
+            if tr:
+                traffic = tr["dram_bytes"] / tr["algorithmic_bytes"] * per_launch_bytes
+                traffic_note = (f"ncu dram__bytes_read+write of one {tr['kernel']} launch ({tr['dram_bytes']:.4g} B for "
+                                f"{tr['algorithmic_bytes']:.4g} algorithmic B), scaled to the class's mean launch")
         except Exception:
             traffic = None
+    tot_ms = max(sum(p["ms"] for p in prof.values()), 1e-9)
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": traffic,
+                "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": traffic, "traffic_note": traffic_note,
                 "algorithmic_bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms,
-                "launches_per_step": d["launches"] / args.steps,
-                "share_of_profiled_time": d["ms"] / max(sum(p["ms"] for p in prof.values()), 1e-9),
+                "launches_per_step": d["launches"] / args.steps, "share_of_profiled_time": d["ms"] / tot_ms,
                 "classes": prof}
-    fp32_state = {k: h.get_field(k) for k in ("phi", "psi", "u")}
-    h.close()
+    net_roof = None
+    if prof.get("psi_net", {}).get("launches"):
+        pn = prof["psi_net"]
+        px = 3 * V * kw["Nx"] * kw["Ny"]
+        tf = pn["launches"] * px * NET_FLOP_PER_PIXEL / (pn["ms"] / 1000.0) / 1e12
+        net_roof = {"bound": "tensor", "kernel": "k_net_apply (mma.sync bf16)", "achieved": tf, "peak": tflops_peak,
+                    "unit": "TFLOP/s", "frac": tf / tflops_peak, "ms_per_launch": pn["ms"] / pn["launches"],
+                    "launches_per_step": pn["launches"] / args.steps, "share_of_profiled_time": pn["ms"] / tot_ms,
+                    "flop_per_pixel": NET_FLOP_PER_PIXEL}
 
-    # FP64 reference-form path on the same workload (the plain FP64 diagonal BiCGSTAB GPU solver)
-    k64 = max(1, min(args.steps, 3))
-    h64 = Handle(Cfg(**kw), precision="fp64", psi_form="full", device=local)
-    h64.init_state(phi, psi)
-    h64.run(1, args.warmup, monitor=True)
-    ms64 = h64.time_run(1 + args.warmup, k64, monitor=True)
-    it64 = h64.psi_stats()[:, 0].tolist()
-    h64.close()
-    ms64 = max_over_ranks(ms64, ws)
-    fp64_sps = ws * k64 / (ms64 / 1000.0)
-
-    # accuracy of the mixed and FP32-bulk paths against the FP64 GPU path, same steps;
-    # FP32-bulk speed on the same workload
+    # reference accuracy: the FP64 reference-form solve, same workload and steps
     acc_steps = 3
     hb = Handle(Cfg(**kw), precision="fp64", psi_form="full", device=local)
     hb.init_state(phi, psi)
@@ -323,18 +345,23 @@ def run_ours(args):
         acc["max_field_err"] = max(acc[k] for k in ("phi", "psi", "mu", "nu", "u", "p"))
         return acc
 
-    ha = Handle(Cfg(**kw), **MAIN)
-    ha.init_state(phi, psi)
-    Ea, _ = ha.run(1, acc_steps, monitor=True)
-    acc = errors(ha, Ea)
-    ha.close()
-    hf = Handle(Cfg(**kw), precision="fp32", psi_form="full", psi_rtol=1e-8, psi_itmax=60, device=local)
-    hf.init_state(phi, psi)
-    Ef, _ = hf.run(1, acc_steps, monitor=True)
-    acc32 = errors(hf, Ef)
-    ms32 = hf.time_run(1 + acc_steps, k64, monitor=True)
-    hf.close()
-    ms32 = max_over_ranks(ms32, ws)
+    # every configuration: accuracy after acc_steps, then k64 timed steps
+    k64 = max(1, min(args.steps, 3))
+    arms = {}
+    for name, opts in ARMS.items():
+        if args.arms and name not in args.arms.split(","):
+            continue
+        ha = Handle(Cfg(**kw), device=local, **opts)
+        ha.init_state(phi, psi)
+        Ea, _ = ha.run(1, acc_steps, monitor=True)
+        acc = errors(ha, Ea)
+        it_acc = ha.psi_stats()[:, 0].tolist()
+        msa = ha.time_run(1 + acc_steps, k64, monitor=True)
+        msa = max_over_ranks(msa, ws)
+        arms[name] = {"value": ws * k64 / (msa / 1000.0), "unit": "steps/s", "steps": k64,
+                      "psi_iters_last_step": ha.psi_stats()[:, 0].tolist(), "psi_iters_step3": it_acc,
+                      "rel_err_vs_fp64": acc, "options": {k: v for k, v in opts.items() if k != "psi_net"}}
+        ha.close()
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -343,21 +370,26 @@ def run_ours(args):
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-               "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
+               "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32+bf16", "data": "synthetic",
                "config": {"workload": WORKLOAD, "grid": [1024, 1024], "vesicles": V, "runs_per_gpu": 1,
-                          "dt": DT, "precision": "FP32 fields/FFTs, FP64 SAV dots + 3x3 + Q",
-                          "psi_solver": "BiCGSTAB, reference full-spectrum form, diagonal spectral preconditioner, rtol 1e-8",
+                          "dt": DT, "arm": head,
+                          "precision": "FP64 fields, FFTs and SAV scalars; psi BiCGSTAB in FP32 with FP64 "
+                                       "iterative refinement (2 sweeps, inner relative residual 1e-6)",
+                          "psi_solver": {"learned": "flexible BiCGSTAB, diagonal + learned correction (BF16 "
+                                                    "tensor-core network)",
+                                         "flex_diag": "flexible BiCGSTAB, diagonal",
+                                         "mixed_krylov_diag": "Krylov.jl-form BiCGSTAB, diagonal",
+                                         "fp64_diag": "FP64 Krylov.jl-form BiCGSTAB, diagonal",
+                                         "fp32_bulk_learned": "FP32 fields, flexible learned"}[head],
                           "parallelism": f"replicas x{ws}",
                           "l2": "inputs larger than L2 (device state ~3 GB per run)",
                           "step": "Steps 1-7 + update + modified energy + area ratio"},
                "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks, "roofline": roofline,
-               "cpu_baseline": cpu,
-               "psi_iters_last_step": iters,
-               "fp64_diag_gpu": {"value": fp64_sps, "unit": "steps/s", "steps": k64, "psi_iters_last_step": it64},
-               "speedup_vs_fp64_diag": value / fp64_sps,
-               "rel_err_vs_fp64": acc,
-               "fp32_bulk": {"value": ws * k64 / (ms32 / 1000.0), "unit": "steps/s", "steps": k64,
-                             "rel_err_vs_fp64": acc32}}
+               "roofline_net": net_roof, "cpu_baseline": cpu, "psi_iters_last_step": iters, "arms": arms}
+        if "fp64_diag" in arms:
+            out["speedup_vs_fp64_diag"] = value / arms["fp64_diag"]["value"]
+        if "flex_diag" in arms:
+            out["speedup_vs_same_solver_diag"] = value / arms["flex_diag"]["value"]
         print(json.dumps(out), flush=True)
     if ws > 1:
         import torch.distributed as dist
@@ -373,6 +405,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--quick", action="store_true", help="main timed region only (for profiler runs)")
+    ap.add_argument("--arm", default="mixed_krylov_diag", choices=list(ARMS),
+                    help="the configuration of the headline value")
+    ap.add_argument("--arms", default="", help="comma-separated subset of the compared configurations")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

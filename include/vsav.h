@@ -138,7 +138,8 @@ int vsav_time_run(vsav_handle* h, int32_t n0, int32_t nsteps, const double* dt, 
  * the algorithmic bytes of the launch: inputs read once, outputs written once).
  * enable: 1 on, 0 off, 2 reset counters.  kclass: 0 FFT column pass, 1 x-pass
  * r2c, 2 x-pass c2r, 3 x-pass c2c, 4 fused psi x-pass (inverse, x M_psi,
- * forward), 5 psi operator combine, 6 pointwise, 7 learned-preconditioner network.
+ * forward), 5 psi operator combine, 6 pointwise, 7 learned-preconditioner network,
+ * 8 FFT column pass of FP32 data (class 0 then counts the FP64 ones).
  * out3 = (launches, total ms, total bytes). */
 int vsav_profile(vsav_handle* h, int32_t enable);
 /* kernels launched by this library so far (all handles) */
@@ -187,19 +188,27 @@ int vsav_net_get_params(vsav_net* net, double* theta, int32_t rounded);
  * multiples of 32; BF16 activations) */
 int vsav_net_forward(vsav_net* net, const float* x, int32_t B, int32_t H, int32_t W, int32_t periodic,
                      int32_t impl, float* out);
-/* loss = 1/2 sum (out - t)^2 and dloss/dtheta (host [7409]), FP32 kernels */
+/* loss_kind 0: loss = 1/2 sum (out - t)^2; 1: the residual-norm loss of
+ * vsav_net_train (square valid crops, unit weights); and dloss/dtheta
+ * (host [7409]), FP32 kernels */
 int vsav_net_grad(vsav_net* net, const float* x, const float* t, int32_t B, int32_t H, int32_t W,
-                  int32_t periodic, double* loss, double* grad);
+                  int32_t periodic, int32_t loss_kind, double op_c0, double* loss, double* grad);
 /* nsteps Adam steps (betas 0.9/0.999, eps 1e-8, learning rate lr) on
  * minibatches of `batch` crops drawn with replacement (seeded) from the crop
  * sets x [ncrops][2][S][S] and t [ncrops][1][S-10][S-10] (device pointers,
- * valid convolutions), minimising sum (out - t)^2 / sum t^2 of the batch;
- * that loss per step is written to losses[nsteps] (host, may be NULL). */
-int vsav_net_train(vsav_net* net, const float* x, const float* t, int64_t ncrops, int32_t S, int32_t batch,
-                   int32_t nsteps, double lr, uint64_t seed, double* losses);
-/* sum (out - t)^2 / sum t^2 over a whole crop set, in chunks of `batch` */
-int vsav_net_eval(vsav_net* net, const float* x, const float* t, int64_t ncrops, int32_t S, int32_t batch,
-                  double* loss);
+ * valid convolutions), minimising sum_b w_b sum (out - t)^2 / sum_b w_b sum t^2
+ * over the batch, w [ncrops] per-crop weights (device, NULL: all 1).  flip != 0
+ * multiplies input channel 0 and the target of each drawn crop by a random
+ * sign.  loss_kind 1 replaces out - t by the residual it leaves, L(out - t)
+ * with L u = op_c0 u - div_h(M grad_h u) in grid units (5-point conservative
+ * stencil, M = 0.075 + 0.025 * input channel 1), at interior output points.
+ * The loss per step is written to losses[nsteps] (host, may be NULL). */
+int vsav_net_train(vsav_net* net, const float* x, const float* t, const float* w, int64_t ncrops, int32_t S,
+                   int32_t batch, int32_t nsteps, double lr, uint64_t seed, int32_t flip, int32_t loss_kind,
+                   double op_c0, double* losses);
+/* the same weighted loss over a whole crop set, in chunks of `batch` */
+int vsav_net_eval(vsav_net* net, const float* x, const float* t, const float* w, int64_t ncrops, int32_t S,
+                  int32_t batch, int32_t loss_kind, double op_c0, double* loss);
 
 /* Network parameters (theta[7409], layout above) of the learned psi
  * preconditioner of a handle created with psi_precond = 2 (precision FP32 or

@@ -57,13 +57,15 @@ uint64_t splitmix(uint64_t& s) {
   return z ^ (z >> 31);
 }
 
-// normalised loss of the current network on crops [c0, c0 + B) of a set
-void batch_loss(vsav_net* h, const float* x, const float* t, long long c0, int B, int S, double* se, double* st2) {
+// weighted loss sums of the current network on crops [c0, c0 + B) of a set
+void batch_loss(vsav_net* h, const float* x, const float* t, const float* w, long long c0, int B, int S, int kind,
+                float op_c0, double* se, double* st2) {
   Net& n = h->n;
   const long long per_in = 2LL * S * S, per_out = (long long)(S - 10) * (S - 10);
   VSAV_CUDA(cudaMemcpyAsync(n.act[0], x + c0 * per_in, (size_t)B * per_in * 4, cudaMemcpyDefault, n.st));
   n.forward<false>(B, S, S);
-  n.loss(t + c0 * per_out, (long long)B * per_out, 1, n.g0);
+  if (kind == 1) n.loss_res(t + c0 * per_out, B, S, op_c0, n.g0, n.g1, w ? w + c0 : nullptr);
+  else n.loss(t + c0 * per_out, (long long)B * per_out, 1, n.g0, w ? w + c0 : nullptr, per_out);
   double ls[2];
   VSAV_CUDA(cudaMemcpyAsync(ls, n.lsum, 16, cudaMemcpyDeviceToHost, n.st));
   VSAV_CUDA(cudaStreamSynchronize(n.st));
@@ -154,7 +156,7 @@ int vsav_net_forward(vsav_net* h, const float* x, int32_t B, int32_t H, int32_t 
 }
 
 int vsav_net_grad(vsav_net* h, const float* x, const float* t, int32_t B, int32_t H, int32_t W, int32_t periodic,
-                  double* loss, double* grad) {
+                  int32_t loss_kind, double op_c0, double* loss, double* grad) {
   return nguard(h, [&] {
     Net& n = h->n;
     const bool P = periodic != 0;
@@ -163,8 +165,10 @@ int vsav_net_grad(vsav_net* h, const float* x, const float* t, int32_t B, int32_
     const long long no = (long long)B * Ho * Wo;
     VSAV_CUDA(cudaMemcpyAsync(n.act[0], x, (size_t)B * 2 * H * W * 4, cudaMemcpyDefault, n.st));
     VSAV_CUDA(cudaMemcpyAsync(h->tbuf, t, (size_t)no * 4, cudaMemcpyDefault, n.st));
+    if (loss_kind == 1 && (P || H != W)) throw std::runtime_error("the residual loss takes square valid crops");
     if (P) n.forward<true>(B, H, W); else n.forward<false>(B, H, W);
-    n.loss(h->tbuf, no, 0, n.g1);
+    if (loss_kind == 1) n.loss_res(h->tbuf, B, H, (float)op_c0, n.g0, n.g1);
+    else n.loss(h->tbuf, no, 0, n.g1);
     // g1 holds the output gradient; backward uses g0/g1 as ping-pong, so move it
     float* gout = h->tbuf;
     VSAV_CUDA(cudaMemcpyAsync(gout, n.g1, (size_t)no * 4, cudaMemcpyDeviceToDevice, n.st));
@@ -174,15 +178,16 @@ int vsav_net_grad(vsav_net* h, const float* x, const float* t, int32_t B, int32_
     VSAV_CUDA(cudaMemcpyAsync(ls, n.lsum, 16, cudaMemcpyDeviceToHost, n.st));
     VSAV_CUDA(cudaMemcpyAsync(g.data(), n.grad, NET_NPARAM * 4, cudaMemcpyDeviceToHost, n.st));
     VSAV_CUDA(cudaStreamSynchronize(n.st));
-    if (loss) *loss = 0.5 * ls[0];
+    if (loss) *loss = loss_kind == 1 ? ls[0] / std::max(ls[1], 1e-300) : 0.5 * ls[0];
     if (grad)
       for (int k = 0; k < NET_NPARAM; ++k) grad[k] = g[k];
     return VSAV_OK;
   });
 }
 
-int vsav_net_train(vsav_net* h, const float* x, const float* t, int64_t ncrops, int32_t S, int32_t batch, int32_t nsteps,
-                   double lr, uint64_t seed, double* losses) {
+int vsav_net_train(vsav_net* h, const float* x, const float* t, const float* w, int64_t ncrops, int32_t S,
+                   int32_t batch, int32_t nsteps, double lr, uint64_t seed, int32_t flip, int32_t loss_kind,
+                   double op_c0, double* losses) {
   return nguard(h, [&] {
     Net& n = h->n;
     if (!x || !t || ncrops <= 0 || batch <= 0 || nsteps < 0) throw std::runtime_error("bad training arguments");
@@ -190,19 +195,27 @@ int vsav_net_train(vsav_net* h, const float* x, const float* t, int64_t ncrops, 
     if (batch > n.cap_batch) throw std::runtime_error("batch too large");
     const long long per_in = 2LL * S * S, per_out = (long long)(S - 10) * (S - 10);
     std::vector<int> idx(batch);
+    std::vector<float> sg(batch, 1.f);
     std::vector<double> ls(2 * (size_t)std::max(nsteps, 1));
     double* dls = nullptr;
     VSAV_CUDA(cudaMalloc(&dls, ls.size() * sizeof(double)));
     uint64_t s = seed;
     try {
       for (int it = 0; it < nsteps; ++it) {
-        for (int b = 0; b < batch; ++b) idx[b] = (int)(splitmix(s) % (uint64_t)ncrops);
+        for (int b = 0; b < batch; ++b) {
+          idx[b] = (int)(splitmix(s) % (uint64_t)ncrops);
+          if (flip) sg[b] = (splitmix(s) & 1) ? -1.f : 1.f;
+        }
         VSAV_CUDA(cudaMemcpyAsync(n.idx, idx.data(), batch * sizeof(int), cudaMemcpyHostToDevice, n.st));
-        k_gather_crops<<<592, 256, 0, n.st>>>(x, n.idx, batch, per_in, n.act[0]); VSAV_COUNT_LAUNCH();
-        k_gather_crops<<<592, 256, 0, n.st>>>(t, n.idx, batch, per_out, h->tbuf); VSAV_COUNT_LAUNCH();
+        VSAV_CUDA(cudaMemcpyAsync(n.sgn, sg.data(), batch * sizeof(float), cudaMemcpyHostToDevice, n.st));
+        const float* sgn = flip ? n.sgn : nullptr;
+        k_gather_crops<<<592, 256, 0, n.st>>>(x, n.idx, sgn, batch, per_in, (long long)S * S, n.act[0]); VSAV_COUNT_LAUNCH();
+        k_gather_crops<<<592, 256, 0, n.st>>>(t, n.idx, sgn, batch, per_out, per_out, h->tbuf); VSAV_COUNT_LAUNCH();
+        if (w) { k_gather_vals<<<(batch + 255) / 256, 256, 0, n.st>>>(w, n.idx, batch, n.wb_batch); VSAV_COUNT_LAUNCH(); }
         VSAV_LAUNCH_CHECK();
         n.forward<false>(batch, S, S);
-        n.loss(h->tbuf, (long long)batch * per_out, 1, n.g1);
+        if (loss_kind == 1) n.loss_res(h->tbuf, batch, S, (float)op_c0, n.g0, n.g1, w ? n.wb_batch : nullptr);
+        else n.loss(h->tbuf, (long long)batch * per_out, 1, n.g1, w ? n.wb_batch : nullptr, per_out);
         VSAV_CUDA(cudaMemcpyAsync(dls + 2 * it, n.lsum, 16, cudaMemcpyDeviceToDevice, n.st));
         VSAV_CUDA(cudaMemcpyAsync(h->tbuf, n.g1, (size_t)batch * per_out * 4, cudaMemcpyDeviceToDevice, n.st));
         n.backward<false>(h->tbuf, batch, S, S);
@@ -224,14 +237,15 @@ int vsav_net_train(vsav_net* h, const float* x, const float* t, int64_t ncrops, 
   });
 }
 
-int vsav_net_eval(vsav_net* h, const float* x, const float* t, int64_t ncrops, int32_t S, int32_t batch, double* loss) {
+int vsav_net_eval(vsav_net* h, const float* x, const float* t, const float* w, int64_t ncrops, int32_t S, int32_t batch,
+                  int32_t loss_kind, double op_c0, double* loss) {
   return nguard(h, [&] {
     if (!x || !t || ncrops <= 0 || batch <= 0 || !loss) throw std::runtime_error("bad evaluation arguments");
     h->n.check(batch, S, S, false);
     double se = 0.0, st2 = 0.0;
     for (long long c0 = 0; c0 < ncrops; c0 += batch) {
       int b = (int)std::min<long long>(batch, ncrops - c0);
-      batch_loss(h, x, t, c0, b, S, &se, &st2);
+      batch_loss(h, x, t, w, c0, b, S, loss_kind, (float)op_c0, &se, &st2);
     }
     *loss = se / std::max(st2, 1e-300);
     return VSAV_OK;

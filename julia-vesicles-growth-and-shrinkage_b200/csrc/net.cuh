@@ -248,15 +248,17 @@ __global__ void k_sum_parts(const float* __restrict__ part, int nblk, int ne, fl
   grad[e] = (float)s;
 }
 
-// partial sums of (out - t)^2 and t^2 (FP64)
+// partial sums of w (out - t)^2 and w t^2 (FP64); w = wsample[k / per] (1 if NULL)
 __global__ void __launch_bounds__(256) k_loss_parts(const float* __restrict__ out, const float* __restrict__ t, long long n,
+                                                    const float* __restrict__ wsample, long long per,
                                                     double2* __restrict__ part) {
   __shared__ double smm[2 * 2 * 8];
   KSum acc[2] = {{0, 0}, {0, 0}};
   for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const double w = wsample ? (double)wsample[k / per] : 1.0;
     double d = (double)out[k] - (double)t[k];
-    acc[0].add(d * d);
-    acc[1].add((double)t[k] * (double)t[k]);
+    acc[0].add(w * d * d);
+    acc[1].add(w * (double)t[k] * (double)t[k]);
   }
   block_reduce_store<2>(acc, part + 2 * blockIdx.x, smm);
 }
@@ -267,12 +269,80 @@ __global__ void k_loss_fin(const double2* __restrict__ part, int nb, double* __r
   lsum[0] = a.val();
   lsum[1] = b.val();
 }
-// g = scale (out - t), scale = 2 / sum t^2 (normalised) or 1 (plain 1/2 sum (out-t)^2)
+// g = scale w (out - t), scale = 2 / sum w t^2 (normalised) or 1 (plain 1/2 sum (out-t)^2)
 __global__ void k_loss_grad(const float* __restrict__ out, const float* __restrict__ t, long long n,
-                            const double* __restrict__ lsum, int normalised, float* __restrict__ g) {
+                            const float* __restrict__ wsample, long long per, const double* __restrict__ lsum,
+                            int normalised, float* __restrict__ g) {
   const float sc = normalised ? (float)(2.0 / fmax(lsum[1], 1e-300)) : 1.f;
   for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
-    g[k] = sc * (out[k] - t[k]);
+    g[k] = sc * (wsample ? wsample[k / per] : 1.f) * (out[k] - t[k]);
+}
+
+// ---------------------------------------------------------------------------
+// residual-norm loss of valid-convolution crops.  The preconditioner's error
+// out - t is weighted by the psi operator in grid units,
+//   L u = c0 u - div_h(M grad_h u)
+// (conservative 5-point stencil, face coefficient = mean of the two cells,
+// M = 0.075 + 0.025 * input channel 1 of the crop at offset 5), evaluated at
+// the interior output points: the loss is the residual that the corrected
+// preconditioner leaves, sum w |L(out - t)|^2 / sum w |L t|^2.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float crop_M(const float* __restrict__ x, int b, int S, int oy, int ox) {
+  return 0.075f + 0.025f * x[((long long)(2 * b + 1) * S + oy + 5) * S + ox + 5];
+}
+__global__ void __launch_bounds__(256) k_loss_res_parts(const float* __restrict__ out, const float* __restrict__ t,
+                                                        const float* __restrict__ x, int B, int S, float c0,
+                                                        const float* __restrict__ wsample, float* __restrict__ R,
+                                                        double2* __restrict__ part) {
+  __shared__ double smm[2 * 2 * 8];
+  KSum acc[2] = {{0, 0}, {0, 0}};
+  const int Ho = S - 10;
+  const long long per = (long long)Ho * Ho, n = (long long)B * per;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const int b = (int)(k / per), r = (int)(k - (long long)b * per), oy = r / Ho, ox = r - oy * Ho;
+    float res = 0.f;
+    if (oy > 0 && oy < Ho - 1 && ox > 0 && ox < Ho - 1) {
+      const float mc = crop_M(x, b, S, oy, ox);
+      const float me = 0.5f * (mc + crop_M(x, b, S, oy, ox + 1)), mw = 0.5f * (mc + crop_M(x, b, S, oy, ox - 1));
+      const float mn = 0.5f * (mc + crop_M(x, b, S, oy + 1, ox)), ms = 0.5f * (mc + crop_M(x, b, S, oy - 1, ox));
+      const long long c = k;
+      auto Lop = [&](const float* f, bool diff) {
+        auto u = [&](long long j) { return diff ? out[j] - t[j] : t[j]; };
+        const float uc = u(c);
+        return c0 * uc - (me * (u(c + 1) - uc) - mw * (uc - u(c - 1)) + mn * (u(c + Ho) - uc) - ms * (uc - u(c - Ho)));
+      };
+      res = Lop(out, true);
+      const float lt = Lop(t, false);
+      const double w = wsample ? (double)wsample[b] : 1.0;
+      acc[0].add(w * (double)res * res);
+      acc[1].add(w * (double)lt * lt);
+    }
+    R[k] = res;
+  }
+  block_reduce_store<2>(acc, part + 2 * blockIdx.x, smm);
+}
+// g = 2 w L^T R / sum w |L t|^2
+__global__ void k_loss_res_grad(const float* __restrict__ R, const float* __restrict__ x, int B, int S, float c0,
+                                const float* __restrict__ wsample, const double* __restrict__ lsum, float* __restrict__ g) {
+  const int Ho = S - 10;
+  const long long per = (long long)Ho * Ho, n = (long long)B * per;
+  const float sc = (float)(2.0 / fmax(lsum[1], 1e-300));
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const int b = (int)(k / per), r = (int)(k - (long long)b * per), oy = r / Ho, ox = r - oy * Ho;
+    const float mc = crop_M(x, b, S, oy, ox);
+    float diag = c0, off = 0.f;
+    const int dy[4] = {0, 0, 1, -1}, dx[4] = {1, -1, 0, 0};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int ny = oy + dy[q], nx = ox + dx[q];
+      if (ny < 0 || ny >= Ho || nx < 0 || nx >= Ho) continue;
+      const float m = 0.5f * (mc + crop_M(x, b, S, ny, nx));
+      diag += m;
+      off += m * R[k + (long long)dy[q] * Ho + dx[q]];
+    }
+    const float w = wsample ? wsample[b] : 1.f;
+    g[k] = sc * w * (diag * R[k] - off);
+  }
 }
 
 __device__ __forceinline__ bool net_is_weight(int k) {
@@ -302,14 +372,23 @@ __global__ void k_round_params(const float* __restrict__ th, float* __restrict__
   wb[k] = net_is_weight(k) ? bf16_round(th[k]) : th[k];
 }
 
-// crops of a [n][C][Hs][Ws] set into a contiguous batch (index list on the device)
-__global__ void k_gather_crops(const float* __restrict__ src, const int* __restrict__ idx, int B, long long per,
-                               float* __restrict__ dst) {
+// crops of a [n][C][Hs][Ws] set into a contiguous batch (index list on the
+// device); the first nflip values of crop b are multiplied by sgn[b] (sign
+// augmentation; sgn NULL: none)
+__global__ void k_gather_crops(const float* __restrict__ src, const int* __restrict__ idx, const float* __restrict__ sgn,
+                               int B, long long per, long long nflip, float* __restrict__ dst) {
   long long tot = (long long)B * per;
   for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < tot; k += (long long)gridDim.x * blockDim.x) {
     long long b = k / per, r = k - b * per;
-    dst[k] = src[(long long)idx[b] * per + r];
+    float v = src[(long long)idx[b] * per + r];
+    if (sgn && r < nflip) v *= sgn[b];
+    dst[k] = v;
   }
+}
+// per-sample values of a batch: dst[b] = src[idx[b]]
+__global__ void k_gather_vals(const float* __restrict__ src, const int* __restrict__ idx, int B, float* __restrict__ dst) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < B) dst[b] = src[idx[b]];
 }
 
 // ---------------------------------------------------------------------------
@@ -322,6 +401,7 @@ struct Net {
   double2* lpart = nullptr;
   double* lsum = nullptr;
   int* idx = nullptr;
+  float *sgn = nullptr, *wb_batch = nullptr;
   long long cap_pix = 0;          // max B*H*W of an input batch
   int cap_batch = 0;
   int nblk_w = 0, nblk_loss = 0;
@@ -352,6 +432,8 @@ struct Net {
     lpart = alloc<double2>(2 * nblk_loss);
     lsum = alloc<double>(2);
     idx = alloc<int>(cap_batch);
+    sgn = alloc<float>(cap_batch);
+    wb_batch = alloc<float>(cap_batch);
     VSAV_CUDA(cudaMemsetAsync(theta, 0, NET_NPARAM * 4, st));
     reset_opt();
     k_round_params<<<(NET_NPARAM + 255) / 256, 256, 0, st>>>(theta, wb); VSAV_COUNT_LAUNCH();
@@ -438,11 +520,19 @@ struct Net {
       }
     }
   }
-  // loss of act[NET_NL] against t (n values); gradient into g1 region reserved: uses gl
-  void loss(const float* t, long long n, int normalised, float* gl) {
-    k_loss_parts<<<nblk_loss, 256, 0, st>>>(act[NET_NL], t, n, lpart); VSAV_COUNT_LAUNCH();
+  // loss of act[NET_NL] against t (n values, per-sample weights w over `per`
+  // values each, or NULL); its output gradient into gl
+  void loss(const float* t, long long n, int normalised, float* gl, const float* w = nullptr, long long per = 1) {
+    k_loss_parts<<<nblk_loss, 256, 0, st>>>(act[NET_NL], t, n, w, per, lpart); VSAV_COUNT_LAUNCH();
     k_loss_fin<<<1, 32, 0, st>>>(lpart, nblk_loss, lsum); VSAV_COUNT_LAUNCH();
-    k_loss_grad<<<nblk_loss, 256, 0, st>>>(act[NET_NL], t, n, lsum, normalised, gl); VSAV_COUNT_LAUNCH();
+    k_loss_grad<<<nblk_loss, 256, 0, st>>>(act[NET_NL], t, n, w, per, lsum, normalised, gl); VSAV_COUNT_LAUNCH();
+    VSAV_LAUNCH_CHECK();
+  }
+  // residual-norm loss (valid crops of size S, inputs in act[0]); R in rbuf
+  void loss_res(const float* t, int B, int S, float c0, float* rbuf, float* gl, const float* w = nullptr) {
+    k_loss_res_parts<<<nblk_loss, 256, 0, st>>>(act[NET_NL], t, act[0], B, S, c0, w, rbuf, lpart); VSAV_COUNT_LAUNCH();
+    k_loss_fin<<<1, 32, 0, st>>>(lpart, nblk_loss, lsum); VSAV_COUNT_LAUNCH();
+    k_loss_res_grad<<<nblk_loss, 256, 0, st>>>(rbuf, act[0], B, S, c0, w, lsum, gl); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
   }
   void adam(float lr, float b1 = 0.9f, float b2 = 0.999f, float eps = 1e-8f) {

@@ -138,7 +138,8 @@ __global__ void k_import_hat(const double* src, cplx<T>* dst, int Fo, int Fi, lo
 // handle's stream, plus the algorithmic bytes of each launch (inputs read once
 // + outputs written once).  Off unless enabled.
 // ---------------------------------------------------------------------------
-enum KClass : int { KC_COLS = 0, KC_ROWS_R2C, KC_ROWS_C2R, KC_ROWS_C2C, KC_ROWS_MUL, KC_PSI_VEC, KC_POINTWISE, KC_NET, KC_N };
+enum KClass : int { KC_COLS = 0, KC_ROWS_R2C, KC_ROWS_C2R, KC_ROWS_C2C, KC_ROWS_MUL, KC_PSI_VEC, KC_POINTWISE, KC_NET,
+                    KC_COLS_F32, KC_N };
 
 struct Prof {
   bool on = false;
@@ -511,7 +512,7 @@ class Solver : public SolverBase {
       }
       VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
-      prof.end(st, KC_COLS, cb);
+      prof.end(st, std::is_same<T, float>::value ? KC_COLS_F32 : KC_COLS, cb);
     })
   }
   void rows_mul(C* t, long long nrows, bool full, int f0 = 0, int fc = 0) {

@@ -112,10 +112,11 @@ def load(path: str = LIB_PATH):
         "vsav_net_set_params": ([H, D], ct.c_int),
         "vsav_net_get_params": ([H, D, i32], ct.c_int),
         "vsav_net_forward": ([H, ct.c_void_p, i32, i32, i32, i32, i32, ct.c_void_p], ct.c_int),
-        "vsav_net_grad": ([H, ct.c_void_p, ct.c_void_p, i32, i32, i32, i32, D, D], ct.c_int),
-        "vsav_net_train": ([H, ct.c_void_p, ct.c_void_p, ct.c_int64, i32, i32, i32, ct.c_double, ct.c_uint64, D],
-                           ct.c_int),
-        "vsav_net_eval": ([H, ct.c_void_p, ct.c_void_p, ct.c_int64, i32, i32, D], ct.c_int),
+        "vsav_net_grad": ([H, ct.c_void_p, ct.c_void_p, i32, i32, i32, i32, i32, ct.c_double, D, D], ct.c_int),
+        "vsav_net_train": ([H, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int64, i32, i32, i32, ct.c_double,
+                            ct.c_uint64, i32, i32, ct.c_double, D], ct.c_int),
+        "vsav_net_eval": ([H, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int64, i32, i32, i32, ct.c_double, D],
+                          ct.c_int),
         "vsav_set_psi_net": ([H, D], ct.c_int),
         "vsav_psi_harvest": ([H, i32], ct.c_int),
         "vsav_psi_harvest_read": ([H, ct.c_void_p, ct.c_int64, ct.POINTER(i32), ct.POINTER(ct.c_int64)], ct.c_int),

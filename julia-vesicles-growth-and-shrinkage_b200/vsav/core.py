@@ -219,7 +219,7 @@ class Handle:
         return float(ms[0])
 
     KCLASS = ("fft_cols", "fft_rows_r2c", "fft_rows_c2r", "fft_rows_c2c", "psi_rows_fused", "psi_combine",
-              "pointwise", "psi_net")
+              "pointwise", "psi_net", "fft_cols_f32")
 
     def profile(self, enable):
         self._chk(self.lib.vsav_profile(self.h, {True: 1, False: 0, "reset": 2}[enable]))

@@ -85,27 +85,35 @@ class Net:
         self._chk(self.lib.vsav_net_forward(self.h, _fptr(x), B, H, W, int(periodic), int(fused), _fptr(out)))
         return out
 
-    def grad(self, x: np.ndarray, t: np.ndarray, periodic: bool):
-        """(1/2 sum (out - t)^2, its gradient w.r.t. theta)."""
+    def grad(self, x: np.ndarray, t: np.ndarray, periodic: bool, residual_c0=None):
+        """(1/2 sum (out - t)^2, its gradient w.r.t. theta); with residual_c0
+        the normalised residual-norm loss of train() instead."""
         x = np.ascontiguousarray(x, dtype=np.float32)
         t = np.ascontiguousarray(t, dtype=np.float32)
         B, _, H, W = x.shape
         loss = ct.c_double()
         g = np.empty(n_params())
-        self._chk(self.lib.vsav_net_grad(self.h, _fptr(x), _fptr(t), B, H, W, int(periodic), ct.byref(loss), L.dptr(g)))
+        kind, c0 = (0, 0.0) if residual_c0 is None else (1, float(residual_c0))
+        self._chk(self.lib.vsav_net_grad(self.h, _fptr(x), _fptr(t), B, H, W, int(periodic), kind, c0, ct.byref(loss),
+                                         L.dptr(g)))
         return loss.value, g
 
     def train(self, x_dev: int, t_dev: int, ncrops: int, S: int, batch: int, nsteps: int, lr: float,
-              seed: int = 0) -> np.ndarray:
+              seed: int = 0, w_dev: int = 0, flip: bool = False, residual_c0=None) -> np.ndarray:
         """nsteps Adam steps on device crop sets (addresses of float32
-        [ncrops][2][S][S] and [ncrops][1][S-10][S-10]); per-step normalised loss."""
+        [ncrops][2][S][S] and [ncrops][1][S-10][S-10], optional per-crop loss
+        weights [ncrops]); per-step weighted normalised loss.  residual_c0:
+        use the residual-norm loss with operator constant c0 (grid units)."""
         losses = np.empty(max(nsteps, 1))
-        self._chk(self.lib.vsav_net_train(self.h, ct.c_void_p(x_dev), ct.c_void_p(t_dev), int(ncrops), int(S),
-                                          int(batch), int(nsteps), float(lr), int(seed), L.dptr(losses)))
+        kind, c0 = (0, 0.0) if residual_c0 is None else (1, float(residual_c0))
+        self._chk(self.lib.vsav_net_train(self.h, ct.c_void_p(x_dev), ct.c_void_p(t_dev), ct.c_void_p(w_dev or None),
+                                          int(ncrops), int(S), int(batch), int(nsteps), float(lr), int(seed), int(flip),
+                                          kind, c0, L.dptr(losses)))
         return losses[:nsteps]
 
-    def eval(self, x_dev: int, t_dev: int, ncrops: int, S: int, batch: int) -> float:
+    def eval(self, x_dev: int, t_dev: int, ncrops: int, S: int, batch: int, w_dev: int = 0, residual_c0=None) -> float:
         loss = ct.c_double()
-        self._chk(self.lib.vsav_net_eval(self.h, ct.c_void_p(x_dev), ct.c_void_p(t_dev), int(ncrops), int(S),
-                                         int(batch), ct.byref(loss)))
+        kind, c0 = (0, 0.0) if residual_c0 is None else (1, float(residual_c0))
+        self._chk(self.lib.vsav_net_eval(self.h, ct.c_void_p(x_dev), ct.c_void_p(t_dev), ct.c_void_p(w_dev or None),
+                                         int(ncrops), int(S), int(batch), kind, c0, ct.byref(loss)))
         return loss.value

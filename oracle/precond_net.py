@@ -127,6 +127,62 @@ def forward(theta, x, periodic, keep=False):
     return (a, acts) if keep else a
 
 
+def backward(theta, acts, g, periodic):
+    """Gradients (dtheta, dx) of sum(g * out) given the activations of forward."""
+    layers = unpack(round_weights(theta))
+    grad = np.zeros(n_params())
+    gviews = unpack(grad)
+    for li in range(len(layers) - 1, -1, -1):
+        W, _ = layers[li]
+        dW, db, dx = conv_backward(acts[li], W, g, periodic)
+        gviews[li][0][...] = dW
+        gviews[li][1][...] = db
+        g = dx * (acts[li] > 0) if li > 0 else dx
+    return grad, g
+
+
+def residual_op(u, m, c0):
+    """L u = c0 u - div_h(M grad_h u) in grid units at the interior points of
+    u [B][H][W] (5-point conservative stencil, face M = mean of the two
+    cells; zero on the border)."""
+    R = np.zeros_like(u)
+    c = (slice(None), slice(1, -1), slice(1, -1))
+    uc, mc = u[c], m[c]
+    me = 0.5 * (mc + m[:, 1:-1, 2:]); mw = 0.5 * (mc + m[:, 1:-1, :-2])
+    mn = 0.5 * (mc + m[:, 2:, 1:-1]); ms = 0.5 * (mc + m[:, :-2, 1:-1])
+    R[c] = c0 * uc - (me * (u[:, 1:-1, 2:] - uc) - mw * (uc - u[:, 1:-1, :-2])
+                      + mn * (u[:, 2:, 1:-1] - uc) - ms * (uc - u[:, :-2, 1:-1]))
+    return R
+
+
+def residual_op_adjoint(R, m, c0):
+    """L^T R for residual_op (R zero on the border)."""
+    B, H, W = R.shape
+    g = c0 * R.copy()
+    for dy, dx in ((0, 1), (0, -1), (1, 0), (-1, 0)):
+        # face between x and x + (dy, dx): contributes m_f (R_x - R_{x+d}) to g_x for x, x+d in range
+        ys = slice(max(0, -dy), H - max(0, dy)); xs = slice(max(0, -dx), W - max(0, dx))
+        yn = slice(max(0, dy), H - max(0, -dy)); xn = slice(max(0, dx), W - max(0, -dx))
+        mf = 0.5 * (m[:, ys, xs] + m[:, yn, xn])
+        g[:, ys, xs] += mf * (R[:, ys, xs] - R[:, yn, xn])
+    return g
+
+
+def residual_loss_and_grad(theta, x, t, c0, w=None):
+    """Residual-norm loss of valid crops: sum w |L(out - t)|^2 / sum w |L t|^2,
+    M = 0.075 + 0.025 * input channel 1 at the output points; (L, dL/dtheta)."""
+    out, acts = forward(theta, x, False, keep=True)
+    m = 0.075 + 0.025 * x[:, 1, 5:-5, 5:-5]
+    w = np.ones(x.shape[0]) if w is None else np.asarray(w, float)
+    R = residual_op(out[:, 0] - t[:, 0], m, c0)
+    Lt = residual_op(t[:, 0], m, c0)
+    den = float(np.sum(w[:, None, None] * Lt * Lt))
+    L = float(np.sum(w[:, None, None] * R * R)) / den
+    gout = (2.0 / den) * w[:, None, None] * residual_op_adjoint(R, m, c0)
+    grad, _ = backward(theta, acts, gout[:, None], False)
+    return L, grad
+
+
 def loss_and_grad(theta, x, t, periodic):
     """L = 1/2 sum (out - t)^2; returns (L, dL/dtheta, dL/dx)."""
     layers = unpack(round_weights(theta))

@@ -65,3 +65,36 @@ def test_adam_step():
     th2, m2, v2 = P.adam(th, m, v, g, 1, 0.1)
     # first step of Adam moves every parameter by lr against the gradient sign
     assert np.allclose(th2, th - 0.1 * np.sign(g), atol=1e-6)
+
+
+def test_residual_loss_gradient():
+    """residual_op_adjoint is the transpose of residual_op, and the residual
+    loss gradient matches finite differences."""
+    rng = np.random.default_rng(5)
+    u = rng.standard_normal((2, 7, 9))
+    R = rng.standard_normal((2, 7, 9))
+    R[:, 0, :] = R[:, -1, :] = R[:, :, 0] = R[:, :, -1] = 0
+    m = 0.05 + 0.05 * rng.random((2, 7, 9))
+    assert abs(np.sum(R * P.residual_op(u, m, 0.3)) - np.sum(P.residual_op_adjoint(R, m, 0.3) * u)) < 1e-12
+    th = P.round_weights(P.init_params(1) + 0.01 * rng.standard_normal(P.n_params()))
+    x = rng.standard_normal((2, 2, 16, 17))
+    t = rng.standard_normal((2, 1, 6, 7))
+    w = np.array([1.0, 3.0])
+    L, g = P.residual_loss_and_grad(th, x, t, 0.01, w)
+
+    def Lf(tt):
+        a = x
+        for li, (W, b) in enumerate(P.unpack(tt)):
+            z = P.conv(a, W, b, False)
+            a = np.maximum(z, 0.0) if li < 4 else z
+        m2 = 0.075 + 0.025 * x[:, 1, 5:-5, 5:-5]
+        Rr = P.residual_op(a[:, 0] - t[:, 0], m2, 0.01)
+        Lt = P.residual_op(t[:, 0], m2, 0.01)
+        return np.sum(w[:, None, None] * Rr ** 2) / np.sum(w[:, None, None] * Lt ** 2)
+    assert abs(Lf(th) - L) < 1e-12 * L
+    for k in rng.choice(P.n_params(), 20, replace=False):
+        tp, tm = th.copy(), th.copy()
+        tp[k] += 1e-6
+        tm[k] -= 1e-6
+        fd = (Lf(tp) - Lf(tm)) / 2e-6
+        assert abs(fd - g[k]) <= 1e-5 * max(1.0, abs(g[k])), (k, fd, g[k])
