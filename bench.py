@@ -397,6 +397,87 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_ensemble(args):
+    """Batched ensemble (64 independent runs at 256^2, N ~ U{1..4}, FP32 bulk):
+    one handle advancing all runs with one launch per sub-step, against the
+    same 64 runs solved one after another, each in its own handle."""
+    from vsav import Handle, ics
+    kw, sizes, phi, psi = ics.ensemble(64)
+    opts = dict(precision="fp32", psi_rtol=1e-6, psi_itmax=60)
+    h = Handle(Cfg(**kw), run_sizes=sizes, **opts)
+    h.init_state(phi, psi)
+    h.run(1, args.warmup, monitor=True)
+    ms = h.time_run(1 + args.warmup, args.steps, monitor=True)
+    h.close()
+    R = len(sizes)
+    batched = R * args.steps / (ms / 1000.0)
+    seq_ms = 0.0
+    v0 = 0
+    for r, N in enumerate(sizes):
+        kr = dict(kw, N=N, psi_in_v=kw["psi_in_v"][v0:v0 + N], psi_out_v=kw["psi_out_v"][v0:v0 + N])
+        hr = Handle(Cfg(**kr), **opts)
+        hr.init_state(phi[v0:v0 + N], psi[v0:v0 + N])
+        hr.run(1, args.warmup, monitor=True)
+        seq_ms += hr.time_run(1 + args.warmup, args.steps, monitor=True)
+        hr.close()
+        v0 += N
+    seq = R * args.steps / (seq_ms / 1000.0)
+    print(json.dumps({"workload": "ensemble_256x64", "metric": "aggregate run-steps/s", "unit": "run-steps/s",
+                      "runs": R, "vesicles": int(sum(sizes)), "grid": [256, 256], "precision": "fp32",
+                      "steps": args.steps, "warmup": args.warmup,
+                      "batched": {"value": batched, "ms_per_step": ms / args.steps},
+                      "sequential": {"value": seq, "ms_per_run_step": seq_ms / (R * args.steps)},
+                      "speedup": batched / seq}), flush=True)
+
+
+def run_config(args):
+    """Other configurations of the path, each its own JSON line (not the headline):
+    multi2d_512x4 (2D 512^2, 4 vesicles) and single3d_128 (3D 128^3, spectral-direct
+    psi): FP64 GPU, the faster GPU precision with its per-field error against the
+    FP64 GPU path, and the CPU restatement (oracle) on a bounded sample."""
+    from vsav import Handle, ics
+    from oracle import vsav_oracle as O
+    kw, phi, psi, _ = ics.workload(args.workload, seed=0)
+    # 2D: the headline's dt; 3D: 1e-5 (both inside the range where the oracle's modified energy decreases)
+    kw["dt"] = DT if kw.get("Nz", 0) == 0 else 1e-5
+    fast = "mixed" if args.workload == "multi2d_512x4" else "fp32"
+    out = {"workload": args.workload, "metric": "steps/s", "unit": "steps/s", "steps": args.steps,
+           "warmup": args.warmup, "dt": kw["dt"], "grid": [kw["Nx"], kw["Ny"]] + ([kw["Nz"]] if kw.get("Nz") else []),
+           "vesicles": kw["N"]}
+    ref = None
+    for prec in ("fp64", fast):
+        h = Handle(Cfg(**kw), precision=prec)
+        h.init_state(phi, psi)
+        E, _ = h.run(1, args.warmup, monitor=True)
+        fields = {k: h.get_field(k) for k in ("phi", "psi", "mu", "nu", "u", "p")}
+        ms = h.time_run(1 + args.warmup, args.steps, monitor=True)
+        h.close()
+        res = {"value": args.steps / (ms / 1000.0), "ms_per_step": ms / args.steps,
+               "energy_non_increasing": bool(np.all(np.diff(E[:, 0]) <= 0))}
+        if ref is None:
+            ref = fields
+        else:
+            res["rel_err_vs_fp64_after_warmup_steps"] = {
+                k: float(np.linalg.norm(fields[k] - ref[k]) / max(np.linalg.norm(ref[k]), 1e-300)) for k in ref}
+        out[prec] = res
+    if not args.no_cpu:
+        cfg = O.Config(**kw)
+        cores = os.cpu_count() or 1
+        orc = O.Oracle(cfg, workers=cores)
+        pres = O.make_state(cfg, phi, psi, orc.ops)
+        O.init_state(cfg, pres, orc.ops)
+        old = pres.copy()
+        orc.step(pres, old, 1, kw["dt"])
+        t0 = time.perf_counter()
+        orc.step(pres, old, 2, kw["dt"])
+        orc.monitor(pres, old)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": 1.0 / dt, "unit": "steps/s", "cores": cores, "kind": "port",
+                               "sample": "1 step after 1 warm-up step, FP64 NumPy/pocketfft"}
+        out["speedup_fp64_gpu_vs_cpu"] = out["fp64"]["value"] / out["cpu_baseline"]["value"]
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -408,7 +489,16 @@ def main():
     ap.add_argument("--arm", default="mixed_krylov_diag", choices=list(ARMS),
                     help="the configuration of the headline value")
     ap.add_argument("--arms", default="", help="comma-separated subset of the compared configurations")
+    ap.add_argument("--workload", default="multi2d_1024x8",
+                    choices=["multi2d_1024x8", "ensemble_256x64", "multi2d_512x4", "single3d_128"],
+                    help="anything but multi2d_1024x8 prints its own comparison line, not the headline")
     args = ap.parse_args()
+    if args.workload == "ensemble_256x64":
+        run_ensemble(args)
+        return
+    if args.workload in ("multi2d_512x4", "single3d_128"):
+        run_config(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -69,6 +69,8 @@ typedef struct vsav_options {
   int32_t n_runs;               /* R >= 1 */
   const int32_t* run_sizes;     /* [R] vesicle fields per run (NULL: R == 1 with N fields) */
   int32_t device;               /* CUDA device ordinal */
+  int32_t graph;                /* 1 (default): vsav_run replays each time step after the first as one
+                                   CUDA graph (Krylov loops as conditional nodes); 0: eager launches */
 } vsav_options;
 
 /* field ids (FieldState, src/Types.jl:167-201) */

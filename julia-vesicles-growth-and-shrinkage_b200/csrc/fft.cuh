@@ -244,7 +244,7 @@ __device__ __forceinline__ int tile_fft(C (&v)[E], C* const (&buf)[2], const Lay
 
 // minimum resident CTAs that the register budget must allow, per (E, NT)
 template <int E, int NT> struct MinB {
-  static constexpr int v = (NT >= 512) ? ((E <= 8) ? 2 : 1) : ((E <= 4) ? 4 : ((E <= 8) ? 3 : 2));
+  static constexpr int v = (NT >= 1024) ? 1 : (NT >= 512) ? ((E <= 8) ? 2 : 1) : ((E <= 4) ? 4 : ((E <= 8) ? 3 : 2));
 };
 template <typename T> struct FFTCfg;
 template <> struct FFTCfg<float> { static constexpr int E = 16; static constexpr int CHUNK = 4096; };

@@ -176,12 +176,35 @@ __global__ void __launch_bounds__(256) k_psi_combine(const cplx<T>* __restrict__
   if (act) {
     const double adt = adt_r[r], mm = mmax_r ? mmax_r[r] : 0.0;
     const long long beg = (long long)blockIdx.x * ew.chunk, end = min(ew.n, beg + ew.chunk);
-    for (long long s = beg + threadIdx.x; s < end; s += blockDim.x) {
+    // U elements per thread per round, their loads issued before any use
+    constexpr int U = 4;
+    for (long long s0 = beg + threadIdx.x; s0 < end; s0 += U * blockDim.x) {
+      cplx<T> xv[U], av[U], bv[U], cv[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const long long s = s0 + (long long)u * blockDim.x;
+        if (s < end) {
+          const long long j = (long long)f * g.n + s;
+          xv[u] = x ? x[j] : cplx<T>{};
+          av[u] = t1[j];
+          bv[u] = t2[j];
+          cv[u] = mode == 0 ? cvec[j] : svec[j];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+      const long long s = s0 + (long long)u * blockDim.x;
+      if (s >= end) break;
       int kx, ky; double kxv, kyv, w;
       vk(g, s, kx, ky, kxv, kyv, w);
       if (w == 0.0) continue;
       long long j = (long long)f * g.n + s;
-      double2 o = op_out<T>(g, x, t1, t2, j, kx, kxv, kyv, adt, -1.0);
+      double2 o;
+      {
+        double mx = (!g.full && kx == g.Nx / 2) ? 0.0 : kxv;
+        double2 d = make_double2(-(mx * (double)av[u].y + kyv * (double)bv[u].y), mx * (double)av[u].x + kyv * (double)bv[u].x);
+        o = make_double2(adt * (double)xv[u].x - d.x, adt * (double)xv[u].y - d.y);
+      }
       if (!g.full && (kx == 0 || kx == g.Nx / 2)) {
         int kym = (g.Ny - ky) % g.Ny;
         long long jm = (long long)f * g.n + (long long)kym * g.kp + kx;
@@ -198,14 +221,15 @@ __global__ void __launch_bounds__(256) k_psi_combine(const cplx<T>* __restrict__
       y[j] = ot;
       double ox = ot.x, oy = ot.y;   // use the stored (rounded) values in the dots
       if (mode == 0) {
-        cplx<T> c = cvec[j];
+        const cplx<T> c = cv[u];
         acc[0].add(w * ((double)c.x * ox + (double)c.y * oy));
         if (g.full) acc[1].add((double)c.x * oy - (double)c.y * ox);
       } else {
-        cplx<T> sv = svec[j];
+        const cplx<T> sv = cv[u];
         acc[0].add(w * (ox * (double)sv.x + oy * (double)sv.y));
         if (g.full) acc[1].add(ox * (double)sv.y - oy * (double)sv.x);
         acc[2].add(w * (ox * ox + oy * oy));
+      }
       }
     }
   }

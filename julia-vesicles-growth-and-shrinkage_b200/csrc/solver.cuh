@@ -31,6 +31,7 @@ struct Options {
   int psi_mixed = 0;         // FP64 fields with the psi BiCGSTAB in FP32 + FP64 iterative refinement
   int psi_refine = 2;        // refinement sweeps of the mixed mode
   double psi_inner_rtol = 1e-6;
+  int graph = 1;             // vsav_run replays each time step as a CUDA graph
 };
 
 struct StepStatus {
@@ -62,6 +63,9 @@ class SolverBase {
   virtual void step7(int n) = 0;
   virtual void update_state() = 0;
   virtual void monitor(double* energy, double* aratio) = 0;
+  // one whole time step (Steps 1-7, update, optional monitor) replayed from a CUDA graph
+  // captured on first use; false if this handle runs steps eagerly
+  virtual bool step_graph(int n, double* energy, double* aratio) = 0;
   virtual void get_work(int what, int idx, void* host) = 0;
   virtual void get_scalar_work(int what, double* out) = 0;
   virtual void transform(int kind, int nf, const double* in, double* out) = 0;
@@ -101,6 +105,19 @@ __global__ void k_init_scalars(const double* sch, double* s, int R) {
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r < R) { s[r * 4 + 0] = 1.0; s[r * 4 + 1] = sch[r * 8 + 0]; s[r * 4 + 2] = sch[r * 8 + 1]; s[r * 4 + 3] = sch[r * 8 + 2]; }
   }
+
+// Condition of a Krylov WHILE node of a captured time step: 1 while any
+// system is active.  Bounded: after itmax + 1 evaluations the loop stops
+// whatever the flags say (and flags the overrun in *err, bit 3).
+__global__ void k_loop_cond(cudaGraphConditionalHandle hnd, const BiState* st_, int S, unsigned* trips, int limit,
+                            int* err) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  int any = 0;
+  for (int s = 0; s < S; ++s) any |= st_[s].active;
+  const unsigned t = ++(*trips);
+  if (any && (int)t > limit) { any = 0; atomicOr(err, 8); }
+  cudaGraphSetConditional(hnd, any ? 1u : 0u);
+}
 
 __global__ void k_bi_flags(const BiState* st_, int* upd, int S) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -199,6 +216,19 @@ __global__ void k_sub(const T* __restrict__ b, const T* __restrict__ y, T* __res
 }
 
 template <typename T> class Solver;
+
+// Book-keeping of one step-graph capture: the kernels captured outside the
+// Krylov loops, and per loop (a WHILE node) the kernels of its body and the
+// device counter of its evaluated conditions (1 + iterations).
+struct CaptureCtx {
+  long long fixed = 0;
+  std::vector<long long> body;
+  unsigned* d_trips = nullptr;     // [kMaxLoops]
+  cudaStream_t side = nullptr;     // stream the loop bodies are captured on
+  int* err = nullptr;              // error flags of the handle that owns the capture
+  static constexpr int kMaxLoops = 16;
+};
+inline CaptureCtx*& capture_ctx() { static thread_local CaptureCtx* c = nullptr; return c; }
 
 template <typename T>
 class Solver : public SolverBase {
@@ -368,6 +398,13 @@ class Solver : public SolverBase {
   ~Solver() override {
     cudaStreamSynchronize(st);
     if (hv) cudaFree(hv);
+    for (auto& row : sgraph)
+      for (auto& sg : row) {
+        if (sg.exec) cudaGraphExecDestroy(sg.exec);
+        if (sg.graph) cudaGraphDestroy(sg.graph);
+      }
+    if (side_st) cudaStreamDestroy(side_st);
+    if (h_trips) cudaFreeHost(h_trips);
     if (psi32) { delete psi32; psi32 = nullptr; }
     if (own_stream == false) st = nullptr;
     for (void* p : allocs) cudaFree(p);
@@ -390,11 +427,13 @@ class Solver : public SolverBase {
 
   // ---- FFT kernel variants: (E elements per thread, NT threads per CTA) ----
   // The autotuner picks one variant per pass family at handle creation.
-  enum Fam { FAM_R2C = 0, FAM_C2R, FAM_C2C, FAM_MUL, FAM_COLS, FAM_N };
-  static constexpr int NVAR = 4;
-  static constexpr int VE[2][NVAR] = {{8, 8, 16, 32}, {4, 4, 8, 16}};      // [T==double][variant]
-  static constexpr int VNT[NVAR] = {256, 512, 256, 256};
-  int choice[FAM_N] = {0, 0, 0, 0, 0};
+  // FAM_COLS: column passes of half spectra; FAM_COLS_PSI: of the full-spectrum
+  // psi vectors (2D, 3V or 6V fields), tuned separately
+  enum Fam { FAM_R2C = 0, FAM_C2R, FAM_C2C, FAM_MUL, FAM_COLS, FAM_COLS_PSI, FAM_N };
+  static constexpr int NVAR = 6;
+  static constexpr int VE[2][NVAR] = {{8, 8, 16, 32, 8, 16}, {4, 4, 8, 16, 4, 8}};      // [T==double][variant]
+  static constexpr int VNT[NVAR] = {256, 512, 256, 256, 1024, 512};
+  int choice[FAM_N] = {0, 0, 0, 0, 0, 0};
   bool tuned_from_cache = false;
   double tune_ms[FAM_N][NVAR] = {};
   static constexpr int DIX = std::is_same<T, double>::value ? 1 : 0;
@@ -419,7 +458,9 @@ class Solver : public SolverBase {
     case 0: { constexpr int E_ = VE[DIX][0], NT_ = VNT[0]; __VA_ARGS__; } break;         \
     case 1: { constexpr int E_ = VE[DIX][1], NT_ = VNT[1]; __VA_ARGS__; } break;         \
     case 2: { constexpr int E_ = VE[DIX][2], NT_ = VNT[2]; __VA_ARGS__; } break;         \
-    default: { constexpr int E_ = VE[DIX][3], NT_ = VNT[3]; __VA_ARGS__; } break;        \
+    case 3: { constexpr int E_ = VE[DIX][3], NT_ = VNT[3]; __VA_ARGS__; } break;         \
+    case 4: { constexpr int E_ = VE[DIX][4], NT_ = VNT[4]; __VA_ARGS__; } break;         \
+    default: { constexpr int E_ = VE[DIX][5], NT_ = VNT[5]; __VA_ARGS__; } break;        \
   }
 
   template <int E_, int NT_>
@@ -493,7 +534,7 @@ class Solver : public SolverBase {
   }
   void cols(bool inv, int geo, long long nf, const C* in0, const C* in1, double a0, double a1, int mult, double ms,
             C* out, double oscale) {
-    VSAV_DISPATCH(FAM_COLS, {
+    VSAV_DISPATCH(geo == 3 ? FAM_COLS_PSI : FAM_COLS, {
       long long nouter = nf;
       ColArgs a = colargs(geo, nouter, E_, NT_);
       int L = 1 << a.logL;
@@ -553,11 +594,11 @@ class Solver : public SolverBase {
   bool variant_ok(int fam, int v) const {
     int Lr = (fam == FAM_C2C || (fam == FAM_MUL && psi_full())) ? g.Nx : g.Nx / 2;
     int Lc = (g.nd == 3) ? std::min(g.Ny, g.Nz) : g.Ny;
-    int L = (fam == FAM_COLS) ? Lc : Lr;
+    int L = (fam == FAM_COLS || fam == FAM_COLS_PSI) ? Lc : Lr;
     return vE(v) <= L && vE(v) * VNT[v] / L >= 1;
   }
   void autotune() {
-    if (const char* forced = getenv("VSAV_TUNE")) {      // "c0,c1,c2,c3,c4"
+    if (const char* forced = getenv("VSAV_TUNE")) {      // "c0,c1,c2,c3,c4,c5" (variant per family)
       int k = 0;
       for (const char* q = forced; *q && k < FAM_N; ++q)
         if (*q >= '0' && *q <= '9') { int v = *q - '0'; if (v < NVAR && variant_ok(k, v)) choice[k] = v; ++k; }
@@ -584,7 +625,7 @@ class Solver : public SolverBase {
     bool have_mul = (g.nd == 2) && vt12 != nullptr;
     for (int fam = 0; fam < FAM_N; ++fam) {
       if (fam == FAM_MUL && !have_mul) continue;
-      if (fam == FAM_C2C && !(g.nd == 2 && psi_full())) continue;
+      if ((fam == FAM_C2C || fam == FAM_COLS_PSI) && !(g.nd == 2 && psi_full())) continue;
       double best = 1e30;
       int bestv = 0;
       while (!variant_ok(fam, bestv) && bestv + 1 < NVAR) ++bestv;
@@ -597,6 +638,7 @@ class Solver : public SolverBase {
             case FAM_C2R: rows_c2r(tmpH, tmpP, 1.0, nrows); break;
             case FAM_C2C: rows_c2c<false>(vb, nullptr, vt, 1.0, 3LL * V * g.Ny); break;
             case FAM_MUL: rows_mul(vt12, 2LL * psi_chunk() * g.Ny, psi_full(), 0, psi_chunk()); break;
+            case FAM_COLS_PSI: cols(true, 3, 3LL * V, vb, nullptr, 1, 0, M_ONE, 1, vt, 1); break;
             default: cols(false, g.nd == 2 ? 0 : 1, V, tmpH, nullptr, 1, 0, M_ONE, 1, tmpH, 1); break;
           }
         };
@@ -614,7 +656,7 @@ class Solver : public SolverBase {
     }
     prof.on = was;
     if (getenv("VSAV_VERBOSE")) {
-      const char* nm[FAM_N] = {"rows_r2c", "rows_c2r", "rows_c2c", "rows_mul", "cols"};
+      const char* nm[FAM_N] = {"rows_r2c", "rows_c2r", "rows_c2c", "rows_mul", "cols", "cols_psi"};
       for (int f = 0; f < FAM_N; ++f) for (int v = 0; v < NVAR; ++v) if (!variant_ok(f, v)) tune_ms[f][v] = -1;
       for (int f = 0; f < FAM_N; ++f) {
         fprintf(stderr, "[vsav autotune %s] %-9s", std::is_same<T, double>::value ? "fp64" : "fp32", nm[f]);
@@ -792,15 +834,27 @@ class Solver : public SolverBase {
   }
 
   // old <- present ; present <- new (written into old's storage by steps 6/7) ; physical fields by irfft
-  void update_state() override {
+  void swap_levels() {
     std::swap(phys4[0], phys4[1]); std::swap(hat4[0], hat4[1]);
     std::swap(uphys[0], uphys[1]); std::swap(uhat[0], uhat[1]);
     std::swap(sc[0], sc[1]);
+    parity ^= 1;
+  }
+  void update_state() override {
+    swap_levels();
+    ++steps_done;
     irfft(hat4[0], 4LL * dm.V, phys4[0]);
     irfft(uhat[0], (long long)(g.nd + 1) * dm.R, uphys[0]);
   }
 
   void monitor(double* h_energy, double* h_aratio) override {
+    monitor_kernels();
+    const int R = dm.R;
+    if (h_energy) VSAV_CUDA(cudaMemcpyAsync(h_energy, energy, R * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (h_aratio) VSAV_CUDA(cudaMemcpyAsync(h_aratio, aratio, R * sizeof(double), cudaMemcpyDeviceToHost, st));
+    VSAV_CUDA(cudaStreamSynchronize(st));
+  }
+  void monitor_kernels() {
     const int V = dm.V, R = dm.R;
     const long long VP = (long long)V * g.P, VH = (long long)V * g.H, RP = (long long)R * g.P, RH = (long long)R * g.H;
     const C* ph_p = uhat[0] + g.nd * RH;
@@ -828,9 +882,81 @@ class Solver : public SolverBase {
     fin(3, R, e, fd2);
     k_fin_mon<<<(R + 63) / 64, 64, 0, st>>>(fd, fd2, sc[0], sc[1], d_dt, d_A0, ph, rn, energy, aratio, area); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
-    if (h_energy) VSAV_CUDA(cudaMemcpyAsync(h_energy, energy, R * sizeof(double), cudaMemcpyDeviceToHost, st));
-    if (h_aratio) VSAV_CUDA(cudaMemcpyAsync(h_aratio, aratio, R * sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
+
+  // ------------------------------------------------------------------ step graphs
+  // A BDF2 time step (Steps 1-7, update, optional monitor) is captured once per
+  // (level parity, monitor) -- the two time levels swap by pointer each step,
+  // so even and odd steps bake in different addresses -- and replayed with one
+  // cudaGraphLaunch; its Krylov loops are conditional WHILE nodes, so a step
+  // needs no host round trip.  The first (BDF1) step runs eagerly, which also
+  // sets every kernel's attributes before any capture.
+  struct StepGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    CaptureCtx cx;
+  };
+  StepGraph sgraph[2][2];         // [level parity][monitor]
+  int parity = 0;
+  unsigned* d_trips_all = nullptr;
+  unsigned* h_trips = nullptr;
+  cudaStream_t side_st = nullptr;
+  long long steps_done = 0;
+
+  void capture_step(StepGraph& sg, int n, int mon, unsigned* trips) {
+    sg.cx = CaptureCtx{};
+    sg.cx.d_trips = trips;
+    sg.cx.side = side_st;
+    sg.cx.err = d_err;
+    capture_ctx() = &sg.cx;
+    const long long c0 = launch_counter().load();
+    VSAV_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    try {
+      step1(n); step2(n); step3(); step4(n); step5(n); step6(); step7(n);
+      update_state();
+      if (mon) monitor_kernels();
+    } catch (...) {
+      cudaGraph_t tmp = nullptr;
+      cudaStreamEndCapture(st, &tmp);
+      if (tmp) cudaGraphDestroy(tmp);
+      capture_ctx() = nullptr;
+      throw;
+    }
+    capture_ctx() = nullptr;
+    VSAV_CUDA(cudaStreamEndCapture(st, &sg.graph));
+    long long total = launch_counter().load() - c0, bodies = 0;
+    for (long long b : sg.cx.body) bodies += b;
+    sg.cx.fixed = total - bodies;
+    launch_counter().fetch_sub(total);      // captured, not launched
+    VSAV_CUDA(cudaGraphInstantiate(&sg.exec, sg.graph, 0));
+  }
+
+  bool step_graph(int n, double* h_energy, double* h_aratio) override {
+    if (!opt.graph || n < 2 || steps_done < 1 || prof.on || hv_cap || (psi32 && psi32->prof.on)) return false;
+    const int mon = (h_energy || h_aratio) ? 1 : 0;
+    if (!d_trips_all) {
+      d_trips_all = dalloc<unsigned>(4 * CaptureCtx::kMaxLoops);
+      VSAV_CUDA(cudaMallocHost(&h_trips, CaptureCtx::kMaxLoops * sizeof(unsigned)));
+      VSAV_CUDA(cudaStreamCreateWithFlags(&side_st, cudaStreamNonBlocking));
+    }
+    StepGraph& sg = sgraph[parity][mon];
+    const bool fresh = sg.exec == nullptr;
+    if (fresh) {
+      set_bdf(n);
+      capture_step(sg, n, mon, d_trips_all + (parity * 2 + mon) * CaptureCtx::kMaxLoops);
+    }
+    set_bdf(n);
+    VSAV_CUDA(cudaGraphLaunch(sg.exec, st));
+    if (!fresh) { swap_levels(); ++steps_done; }   // the capture itself ran update_state once
+    const size_t nl = sg.cx.body.size();
+    if (nl) VSAV_CUDA(cudaMemcpyAsync(h_trips, sg.cx.d_trips, nl * sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    if (h_energy) VSAV_CUDA(cudaMemcpyAsync(h_energy, energy, dm.R * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (h_aratio) VSAV_CUDA(cudaMemcpyAsync(h_aratio, aratio, dm.R * sizeof(double), cudaMemcpyDeviceToHost, st));
     VSAV_CUDA(cudaStreamSynchronize(st));
+    long long launched = sg.cx.fixed;
+    for (size_t l = 0; l < nl; ++l) launched += sg.cx.body[l] * (long long)(h_trips[l] > 0 ? h_trips[l] - 1 : 0);
+    launch_counter().fetch_add(launched);
+    return true;
   }
 
   // simulation.jl:22-53
@@ -930,6 +1056,75 @@ class Solver : public SolverBase {
   Solver<float>* psi32 = nullptr;
   void psi_solve_mixed();
 
+  // Runs iter() -- one BiCGSTAB iteration ending in k_bi_beta, which leaves the
+  // activity of every system in bst and d_any -- until no system is active
+  // (at most itmax times: k_bi_beta retires a system at itmax).  Eagerly: a
+  // host loop reading d_any after each iteration.  Under stream capture (a
+  // time-step graph): a conditional WHILE node whose body is one iteration
+  // followed by the condition kernel, bounded by itmax + 1 iterations.
+  template <typename F> void krylov_loop(int itmax, F&& iter) {
+    const int S = 3 * dm.R;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    VSAV_CUDA(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusActive) {
+      for (int it = 0; it < itmax; ++it) {
+        iter();
+        if (opt.check_every_iter) {
+          VSAV_CUDA(cudaMemcpyAsync(h_pinned_any, d_any, sizeof(int), cudaMemcpyDeviceToHost, st));
+          VSAV_CUDA(cudaStreamSynchronize(st));
+          if (!*h_pinned_any) break;
+        }
+        // refresh the activity flags for the operator kernels of the next iteration
+        k_bi_flags<<<(S + 63) / 64, 64, 0, st>>>(bst, bupd, S); VSAV_COUNT_LAUNCH();
+      }
+      return;
+    }
+    CaptureCtx* cx = capture_ctx();
+    if (!cx || (int)cx->body.size() >= CaptureCtx::kMaxLoops)
+      throw std::runtime_error("Krylov loop captured outside a time-step capture");
+    unsigned* trips = cx->d_trips + cx->body.size();
+    int* err = cx->err ? cx->err : d_err;
+    cudaGraph_t gr = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndep = 0;
+    VSAV_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &gr, &deps, &ndep));
+    cudaGraphConditionalHandle hnd;
+    VSAV_CUDA(cudaGraphConditionalHandleCreate(&hnd, gr, 0, cudaGraphCondAssignDefault));
+    VSAV_CUDA(cudaMemsetAsync(trips, 0, sizeof(unsigned), st));
+    k_loop_cond<<<1, 32, 0, st>>>(hnd, bst, S, trips, itmax + 1, err); VSAV_COUNT_LAUNCH();
+    VSAV_LAUNCH_CHECK();
+    VSAV_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &gr, &deps, &ndep));
+    std::vector<cudaGraphNode_t> dv(deps, deps + ndep);
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = hnd;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    VSAV_CUDA(cudaGraphAddNode(&node, gr, dv.data(), dv.size(), &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    VSAV_CUDA(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    cudaStream_t outer = st;
+    st = cx->side;
+    const long long c0 = launch_counter().load();
+    VSAV_CUDA(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    try {
+      iter();
+      k_bi_flags<<<(S + 63) / 64, 64, 0, st>>>(bst, bupd, S); VSAV_COUNT_LAUNCH();
+      k_loop_cond<<<1, 32, 0, st>>>(hnd, bst, S, trips, itmax + 1, err); VSAV_COUNT_LAUNCH();
+      VSAV_LAUNCH_CHECK();
+    } catch (...) {
+      cudaGraph_t tmp = nullptr;
+      cudaStreamEndCapture(st, &tmp);
+      st = outer;
+      throw;
+    }
+    cudaGraph_t done = nullptr;
+    VSAV_CUDA(cudaStreamEndCapture(st, &done));
+    st = outer;
+    cx->body.push_back(launch_counter().load() - c0);
+  }
+
   // BiCGSTAB (Krylov.jl semantics) on b = vb from x0 = 0, result in x
   void psi_krylov(C* x, double rtol, int itmax) {
     if (opt.psi_precond >= 1) { psi_flex(x, rtol, itmax); return; }
@@ -945,7 +1140,7 @@ class Solver : public SolverBase {
     k_bi_init<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, bupd, sm, S, (int)F, opt.psi_atol, rtol, itmax); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     if (hv_cap) { hv_count = 0; harvest_snap(x, vr); }
-    for (int it = 0; it < itmax; ++it) {
+    krylov_loop(itmax, [&]() {
       matvec(vp, vv, 0, nullptr);                       // v = M^-1 A p ; <c, v>
       fin(4, (int)F, e, fd);
       k_bi_alpha<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, sm, S, (int)F); VSAV_COUNT_LAUNCH();
@@ -962,14 +1157,7 @@ class Solver : public SolverBase {
       k_psi_p<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(vp, vr, vv, bst, bupd, sm, e); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
       if (hv_cap && hv_count < hv_cap) harvest_snap(x, vr);
-      if (opt.check_every_iter) {
-        VSAV_CUDA(cudaMemcpyAsync(h_pinned_any, d_any, sizeof(int), cudaMemcpyDeviceToHost, st));
-        VSAV_CUDA(cudaStreamSynchronize(st));
-        if (!*h_pinned_any) break;
-      }
-      // refresh the activity flags for the operator kernels of the next iteration
-      k_bi_flags<<<(S + 63) / 64, 64, 0, st>>>(bst, bupd, S); VSAV_COUNT_LAUNCH();
-    }
+    });
     if (hv_cap) harvest_final(x);
     (void)full;
   }
@@ -999,7 +1187,7 @@ class Solver : public SolverBase {
     fin(4, (int)F, e, fd);
     k_bi_init<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, bupd, sm, S, (int)F, opt.psi_atol, rtol, itmax); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
-    for (int it = 0; it < itmax; ++it) {
+    krylov_loop(itmax, [&]() {
       precond_apply(vp, vph);
       matvec(vph, vv, 0, nullptr, false);               // v = A p^ ; <c, v>
       fin(4, (int)F, e, fd);
@@ -1017,13 +1205,7 @@ class Solver : public SolverBase {
       k_bi_beta<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, bupd, sm, S, (int)F, itmax, d_any); VSAV_COUNT_LAUNCH();
       k_psi_p<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(vp, vr, vv, bst, bupd, sm, e); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
-      if (opt.check_every_iter) {
-        VSAV_CUDA(cudaMemcpyAsync(h_pinned_any, d_any, sizeof(int), cudaMemcpyDeviceToHost, st));
-        VSAV_CUDA(cudaStreamSynchronize(st));
-        if (!*h_pinned_any) break;
-      }
-      k_bi_flags<<<(S + 63) / 64, 64, 0, st>>>(bst, bupd, S); VSAV_COUNT_LAUNCH();
-    }
+    });
   }
 
   // full-spectrum inverse 2D FFT of F = 3V vectors (normalised), in -> out

@@ -76,6 +76,7 @@ void vsav_default_options(vsav_options* o, const vsav_config* cfg) {
   o->n_runs = 1;
   o->run_sizes = nullptr;
   o->device = 0;
+  o->graph = 1;
 }
 
 int vsav_create(const vsav_config* cfg, const vsav_options* opt, vsav_handle** out) {
@@ -122,6 +123,7 @@ int vsav_create(const vsav_config* cfg, const vsav_options* opt, vsav_handle** o
     if (o.precision != VSAV_FP64 && o.precision != VSAV_FP32 && o.precision != VSAV_MIXED)
       throw std::runtime_error("precision must be VSAV_FP64, VSAV_FP32 or VSAV_MIXED");
     so.psi_mixed = (o.precision == VSAV_MIXED && cfg->ndim == 2) ? 1 : 0;
+    so.graph = o.graph ? 1 : 0;
     if (o.precision == VSAV_FP32)
       h->s = new Solver<float>(d, p, so, rs.data(), cfg->psi_in_v, cfg->psi_out_v);
     else
@@ -209,17 +211,29 @@ int vsav_run(vsav_handle* h, int32_t n0, int32_t nsteps, const double* dt, doubl
   return guard(h, [&] {
     if (n0 < 1 || nsteps < 0) throw std::runtime_error("bad step range");
     int worst = VSAV_OK;
+    std::vector<double> e(h->R), a(h->R);
+    const bool mon = energy || area_ratio;
     for (int k = 0; k < nsteps; ++k) {
       if (dt) h->s->set_dt(dt + (size_t)k * h->R);
       int n = n0 + k;
+      // whole step from a CUDA graph (errors of the step are read after it)
+      if (h->s->step_graph(n, mon ? e.data() : nullptr, mon ? a.data() : nullptr)) {
+        int rc = check_status(h, st);
+        if (rc < 0) return rc;
+        if (rc > 0) worst = rc;
+        for (int r = 0; r < h->R; ++r) {
+          if (energy) energy[(size_t)k * h->R + r] = e[r];
+          if (area_ratio) area_ratio[(size_t)k * h->R + r] = a[r];
+        }
+        continue;
+      }
       h->s->step1(n);
       int rc = check_status(h, st);
       if (rc < 0) return rc;
       if (rc > 0) worst = rc;
       h->s->step2(n); h->s->step3(); h->s->step4(n); h->s->step5(n); h->s->step6(); h->s->step7(n);
       h->s->update_state();
-      if (energy || area_ratio) {
-        std::vector<double> e(h->R), a(h->R);
+      if (mon) {
         h->s->monitor(e.data(), a.data());
         for (int r = 0; r < h->R; ++r) {
           if (energy) energy[(size_t)k * h->R + r] = e[r];

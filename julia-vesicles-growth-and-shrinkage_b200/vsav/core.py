@@ -35,7 +35,7 @@ class Handle:
     def __init__(self, cfg, precision: str = "fp64", psi_form: Optional[str] = None,
                  run_sizes: Optional[Sequence[int]] = None, psi_itmax: int = 20,
                  psi_rtol: Optional[float] = None, psi_atol: float = 1e-14, device: int = 0,
-                 psi_precond: str = "diag", psi_net=None):
+                 psi_precond: str = "diag", psi_net=None, graph: bool = True):
         """cfg: any object with the reference Config fields (Types.jl:27-74);
         psi_in_v / psi_out_v hold one value per vesicle field of all runs.
         psi_precond: "diag" (the reference's left-preconditioned BiCGSTAB),
@@ -71,6 +71,7 @@ class Handle:
         o.precision = PRECISION[precision]
         o.psi_form = PSI_FORM[self.psi_form]
         o.psi_precond = PSI_PRECOND[psi_precond]
+        o.graph = 1 if graph else 0
         self.psi_precond = psi_precond
         o.psi_itmax = psi_itmax
         o.psi_rtol = cfg.tol if psi_rtol is None else psi_rtol

@@ -145,6 +145,24 @@ def single3d(n: int = 128, eps: float = 0.1, seed: int = 0, axes=(1.2, 0.9, 0.7)
     return phi, psi
 
 
+def ensemble(n_runs: int = 64, n: int = 256, eps: float = 0.08, seed: int = 0, nmin: int = 1, nmax: int = 4,
+             dt: float = 1e-6):
+    """Batched ensemble: n_runs independent 2D runs at n^2, each with N ~ U{nmin..nmax}
+    seeded vesicles (multi2d shapes), inside psi U[0.3, 0.9].  Returns (config kwargs
+    with per-field psi_in_v/psi_out_v, run_sizes, phi [V][n][n], psi [V][n][n]);
+    C2 is sized for the largest run (the constant is shared by the handle)."""
+    rng = np.random.default_rng(seed)
+    sizes = [int(k) for k in rng.integers(nmin, nmax + 1, size=n_runs)]
+    phis, psis, tin = [], [], []
+    for r, N in enumerate(sizes):
+        phi, psi, _ = multi2d(n, N, eps, seed * 1000 + r, 0.3, 0.9)
+        phis.append(phi)
+        psis.append(psi)
+        tin += [0.65 if k % 2 == 0 else 0.1 for k in range(N)]
+    kw = params(eps, max(sizes), tin, [0.8] * len(tin), dt, 100 * dt, n, n)
+    return kw, sizes, np.concatenate(phis), np.concatenate(psis)
+
+
 # ---------------------------------------------------------------------------
 # the five benchmark workloads
 # ---------------------------------------------------------------------------

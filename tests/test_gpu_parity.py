@@ -300,3 +300,33 @@ def test_mixed_precision_vs_golden(name):
     np.testing.assert_allclose(h.get_scalars()[0], g["scalars"], rtol=1e-9)
     np.testing.assert_allclose(E[:, 0], g["energy"], rtol=1e-9)
     h.close()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_step_graph_matches_eager(prec):
+    """vsav_run replays steps 2.. as CUDA graphs (Krylov loops as conditional
+    WHILE nodes): same results as the eager launches, bit for bit, the same
+    BiCGSTAB iteration counts, and the same number of kernels executed."""
+    from vsav import _lib
+    kw, g = load_golden("multi2d_n64_N2")
+    out = {}
+    for graph in (False, True):
+        h = make(kw, precision=prec, graph=graph)
+        h.init_state(g["phi0"], g["psi0"])
+        h.run(1, 1, monitor=True)                   # BDF1 step: always eager
+        c0 = _lib.load().vsav_launch_count()
+        E, A = h.run(2, 4, monitor=True)
+        launches = _lib.load().vsav_launch_count() - c0
+        out[graph] = ({k: h.get_field(k) for k in FIELDS}, h.get_scalars(), E, A, h.psi_stats(), launches)
+        h.close()
+    fe, se, Ee, Ae, pe, le = out[False]
+    fg, sg, Eg, Ag, pg, lg = out[True]
+    for k in FIELDS:
+        assert np.array_equal(fe[k], fg[k]), k
+    assert np.array_equal(se, sg) and np.array_equal(Ee, Eg) and np.array_equal(Ae, Ag)
+    assert np.array_equal(pe, pg)
+    # the graph runs the same kernels plus, per Krylov loop, its condition kernel
+    # (once before the loop and once per iteration) and the activity refresh of
+    # the last iteration, which the eager loop skips: iterations + 2 per loop
+    loops = 4 * (1 if prec == "fp64" else 2)
+    assert le < lg <= le + loops * (20 + 2), (le, lg)
