@@ -236,6 +236,144 @@ __global__ void __launch_bounds__(256) k_psi_combine(const cplx<T>* __restrict__
   block_reduce_store<4>(acc, part + ((long long)f * ew.bpf + blockIdx.x) * 4, smm);
 }
 
+// ---------------------------------------------------------------------------
+// FULL-form operator passes fused around the column FFTs
+// ---------------------------------------------------------------------------
+// Inverse y pass for both derivative directions from one read of x:
+//   t1 = IFFT_y(i kx0 S4 x),  t2 = IFFT_y(i ky S4 x)   (x global field f0 + fl,
+// t1/t2 chunk-local field fl).  The second transform re-reads the tile from L2.
+// Fields of inactive systems are skipped (the x pass and the combine skip them).
+template <typename T, int E, int NT>
+__global__ void __launch_bounds__(NT, MinB<E, NT>::v) k_psi_cols_inv2(const cplx<T>* __restrict__ x, cplx<T>* __restrict__ t1,
+                                                                   cplx<T>* __restrict__ t2, double S4, ColArgs a, SysMap sm,
+                                                                   const int* __restrict__ active, int f0,
+                                                                   const cplx<T>* __restrict__ tab) {
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* s = reinterpret_cast<C*>(smraw);
+  const int L = 1 << a.logL, LE = L / E;
+  const int tile = blockIdx.x % a.tiles;
+  const int fl = blockIdx.x / a.tiles;
+  const int f = f0 + fl;
+  if (active && !active[sm.sys(f)]) return;                 // block-uniform
+  const int cl = threadIdx.x & (a.TW - 1), i = threadIdx.x >> a.logTW, c = tile * a.TW + cl;
+  const bool valid = c < a.W;
+  const ColLay lay{a.TW, Log2<E>::v};
+  C* const buf[2] = {s, s + col_tile_elems(L, a.TW, Log2<E>::v)};
+  const C* xin = x + (long long)f * a.O + c;
+#pragma unroll 1
+  for (int d = 0; d < 2; ++d) {
+    const int mult = d == 0 ? M_DX0 : M_DY;
+    C v[E];
+    if (valid) {
+#pragma unroll
+      for (int j = 0; j < E; ++j) v[j] = xin[(long long)(i + j * LE) * a.S] * col_mult<C>(a, mult, S4, c, i + j * LE, 0);
+    } else {
+#pragma unroll
+      for (int j = 0; j < E; ++j) v[j] = mk<C>(0.0, 0.0);
+    }
+    if (d == 1) __syncthreads();                             // the first transform's smem reads are done
+    tile_fft<E, true, true, true>(v, buf, lay, cl, i, true, a.logL, a.logTW, tab);
+    if (valid) {
+      C* o = (d == 0 ? t1 : t2) + (long long)fl * a.O + c;
+#pragma unroll
+      for (int j = 0; j < E; ++j) o[(long long)(i + j * LE) * a.S] = v[j];
+    }
+  }
+}
+
+// Forward y pass of t1 and t2 fused with the operator output, the diagonal
+// preconditioner and the dot products (FULL form; k_psi_combine's modes):
+//   y = P^-1 (a_dt x - (i kx0 t1^ + i ky t2^)),  P^-1 = 1/(a_dt + Mmax S4 k^2) or 1.
+// One block = TW columns of one field; dot partials per (field, tile):
+// part[(f * tiles + tile) * 4 + k].  The transformed t2 tile waits in a third
+// shared-memory area (natural [row][TW] order, each thread its own elements)
+// while t1 is transformed.
+template <typename T, int E, int NT>
+__global__ void __launch_bounds__(NT, MinB<E, NT>::v) k_psi_cols_comb(const cplx<T>* __restrict__ t1, const cplx<T>* __restrict__ t2,
+                                                                   const cplx<T>* __restrict__ x, cplx<T>* __restrict__ y,
+                                                                   const cplx<T>* __restrict__ cvec, const cplx<T>* __restrict__ svec,
+                                                                   int mode, const double* __restrict__ adt_r,
+                                                                   const double* __restrict__ mmax_r, double S4, ColArgs a,
+                                                                   SysMap sm, const int* __restrict__ active, int f0,
+                                                                   const cplx<T>* __restrict__ tab, double2* __restrict__ part) {
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  __shared__ double smm[2 * 4 * (NT / 32)];
+  C* s = reinterpret_cast<C*>(smraw);
+  const int L = 1 << a.logL, LE = L / E;
+  const int tile = blockIdx.x % a.tiles;
+  const int fl = blockIdx.x / a.tiles;
+  const int f = f0 + fl;
+  KSum acc[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+  if (!active || active[sm.sys(f)]) {                       // block-uniform
+    const int cl = threadIdx.x & (a.TW - 1), i = threadIdx.x >> a.logTW, c = tile * a.TW + cl;
+    const bool valid = c < a.W;
+    const ColLay lay{a.TW, Log2<E>::v};
+    C* const buf[2] = {s, s + col_tile_elems(L, a.TW, Log2<E>::v)};
+    C* const res = s + 2 * col_tile_elems(L, a.TW, Log2<E>::v);
+    C v[E];
+    const long long off = (long long)fl * a.O + c;
+#pragma unroll
+    for (int j = 0; j < E; ++j) v[j] = valid ? t2[off + (long long)(i + j * LE) * a.S] : mk<C>(0.0, 0.0);
+    tile_fft<E, false, true, true>(v, buf, lay, cl, i, true, a.logL, a.logTW, tab);
+#pragma unroll
+    for (int j = 0; j < E; ++j) res[(i + j * LE) * a.TW + cl] = v[j];
+#pragma unroll
+    for (int j = 0; j < E; ++j) v[j] = valid ? t1[off + (long long)(i + j * LE) * a.S] : mk<C>(0.0, 0.0);
+    // the operands of the combine, loaded while t1 is transformed (small E only: registers)
+    constexpr int EP = E <= 8 ? E : 1;
+    C xp[EP], cp[EP];
+    const long long gbase = (long long)f * a.O + c;
+    if constexpr (E <= 8) {
+      if (valid) {
+#pragma unroll
+        for (int j = 0; j < E; ++j) {
+          const long long idx = gbase + (long long)(i + j * LE) * a.S;
+          xp[j] = x ? x[idx] : mk<C>(0.0, 0.0);
+          cp[j] = mode == 0 ? cvec[idx] : svec[idx];
+        }
+      }
+    }
+    __syncthreads();                                        // the first transform's smem reads are done
+    tile_fft<E, false, true, true>(v, buf, lay, cl, i, true, a.logL, a.logTW, tab);
+    if (valid) {
+      const int r = sm.run_of[f % sm.V];
+      const double adt = adt_r[r], mm = mmax_r ? mmax_r[r] : 0.0;
+      const double kxv = kfreq(c, a.Nx) * a.kxs;
+#pragma unroll
+      for (int j = 0; j < E; ++j) {
+        const int e = i + j * LE;
+        const double kyv = kfreq(e, a.Ny) * a.kys;
+        const long long idx = gbase + (long long)e * a.S;
+        C xv, cv;
+        if constexpr (E <= 8) { xv = xp[j]; cv = cp[j]; }
+        else { xv = x ? x[idx] : mk<C>(0.0, 0.0); cv = mode == 0 ? cvec[idx] : svec[idx]; }
+        const C w2 = res[e * a.TW + cl];
+        const double dx = -(kxv * (double)v[j].y + kyv * (double)w2.y);
+        const double dy = kxv * (double)v[j].x + kyv * (double)w2.x;
+        double ox = adt * (double)xv.x - dx, oy = adt * (double)xv.y - dy;
+        if (mmax_r) {
+          const double pinv = 1.0 / (adt + mm * S4 * (kxv * kxv + kyv * kyv));
+          ox *= pinv; oy *= pinv;
+        }
+        C ot; ot.x = ox; ot.y = oy;
+        y[idx] = ot;
+        ox = ot.x; oy = ot.y;                               // the dots use the stored (rounded) values
+        if (mode == 0) {
+          acc[0].add((double)cv.x * ox + (double)cv.y * oy);
+          acc[1].add((double)cv.x * oy - (double)cv.y * ox);
+        } else {
+          acc[0].add(ox * (double)cv.x + oy * (double)cv.y);
+          acc[1].add(ox * (double)cv.y - oy * (double)cv.x);
+          acc[2].add(ox * ox + oy * oy);
+        }
+      }
+    }
+  }
+  block_reduce_store<4>(acc, part + ((long long)f * a.tiles + tile) * 4, smm);
+}
+
 // r = M^-1 b, x = 0, p = r, dots <b, r>, ||r||^2  (Krylov.jl bicgstab initialisation)
 template <typename T>
 __global__ void __launch_bounds__(256) k_psi_init(const cplx<T>* __restrict__ b, cplx<T>* __restrict__ x, cplx<T>* __restrict__ r,

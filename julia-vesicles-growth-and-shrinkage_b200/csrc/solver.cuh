@@ -291,6 +291,7 @@ class Solver : public SolverBase {
   Solver(const Dims& d, const Phys& p, const Options& o, const int* run_sizes, const double* psi_in, const double* psi_out)
       : ph(p), opt(o), dm(d) {
     VSAV_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    if (const char* env = getenv("VSAV_PSI_FUSED")) fused_ops = atoi(env) != 0;
     g.nd = d.nd; g.Nx = d.Nx; g.Ny = d.Ny; g.Nz = (d.nd == 3) ? d.Nz : 1;
     g.nkx = d.Nx / 2 + 1;
     g.kp = (g.nkx + 15) / 16 * 16;
@@ -429,11 +430,12 @@ class Solver : public SolverBase {
   // The autotuner picks one variant per pass family at handle creation.
   // FAM_COLS: column passes of half spectra; FAM_COLS_PSI: of the full-spectrum
   // psi vectors (2D, 3V or 6V fields), tuned separately
-  enum Fam { FAM_R2C = 0, FAM_C2R, FAM_C2C, FAM_MUL, FAM_COLS, FAM_COLS_PSI, FAM_N };
-  static constexpr int NVAR = 6;
-  static constexpr int VE[2][NVAR] = {{8, 8, 16, 32, 8, 16}, {4, 4, 8, 16, 4, 8}};      // [T==double][variant]
-  static constexpr int VNT[NVAR] = {256, 512, 256, 256, 1024, 512};
-  int choice[FAM_N] = {0, 0, 0, 0, 0, 0};
+  // FAM_PSI_INV2 / FAM_PSI_COMB: the fused column passes of the FULL psi operator
+  enum Fam { FAM_R2C = 0, FAM_C2R, FAM_C2C, FAM_MUL, FAM_COLS, FAM_COLS_PSI, FAM_PSI_INV2, FAM_PSI_COMB, FAM_N };
+  static constexpr int NVAR = 7;
+  static constexpr int VE[2][NVAR] = {{8, 8, 16, 32, 8, 16, 32}, {4, 4, 8, 16, 4, 8, 16}};      // [T==double][variant]
+  static constexpr int VNT[NVAR] = {256, 512, 256, 256, 1024, 512, 128};
+  int choice[FAM_N] = {0, 0, 0, 0, 0, 0, 0, 0};
   bool tuned_from_cache = false;
   double tune_ms[FAM_N][NVAR] = {};
   static constexpr int DIX = std::is_same<T, double>::value ? 1 : 0;
@@ -460,7 +462,8 @@ class Solver : public SolverBase {
     case 2: { constexpr int E_ = VE[DIX][2], NT_ = VNT[2]; __VA_ARGS__; } break;         \
     case 3: { constexpr int E_ = VE[DIX][3], NT_ = VNT[3]; __VA_ARGS__; } break;         \
     case 4: { constexpr int E_ = VE[DIX][4], NT_ = VNT[4]; __VA_ARGS__; } break;         \
-    default: { constexpr int E_ = VE[DIX][5], NT_ = VNT[5]; __VA_ARGS__; } break;        \
+    case 5: { constexpr int E_ = VE[DIX][5], NT_ = VNT[5]; __VA_ARGS__; } break;         \
+    default: { constexpr int E_ = VE[DIX][6], NT_ = VNT[6]; __VA_ARGS__; } break;        \
   }
 
   template <int E_, int NT_>
@@ -584,6 +587,48 @@ class Solver : public SolverBase {
     })
   }
 
+  // fused FULL-form operator column passes (fields f0 .. f0+fc-1; t1/t2 chunk-local)
+  void psi_cols_inv2(const C* x, C* t1, C* t2, int f0, int fc, bool use_active = true) {
+    SysMap sm{dm.V, dm.R, d_run_of};
+    VSAV_DISPATCH(FAM_PSI_INV2, {
+      long long nouter = fc;
+      ColArgs a = colargs(3, nouter, E_, NT_);
+      int L = 1 << a.logL;
+      int thr = std::max(a.TW, a.TW * L / E_);
+      size_t sm_b = 2 * (size_t)col_tile_elems(L, a.TW, ilog2(E_)) * sizeof(C);
+      long long grid = (long long)a.tiles * fc;
+      set_smem_attr<E_, NT_>((const void*)k_psi_cols_inv2<T, E_, NT_>, sm_b);
+      prof.begin(st);
+      k_psi_cols_inv2<T, E_, NT_><<<(unsigned)grid, thr, sm_b, st>>>(x, t1, t2, ph.S4, a, sm, use_active ? bupd : nullptr, f0, tab);
+      VSAV_COUNT_LAUNCH();
+      VSAV_LAUNCH_CHECK();
+      prof.end(st, std::is_same<T, float>::value ? KC_COLS_F32 : KC_COLS, (double)fc * g.Pfull * 3.0 * sizeof(C));
+    })
+  }
+  // returns the number of dot partials per field (column tiles)
+  int psi_cols_comb(const C* t1, const C* t2, const C* x, C* y, int mode, const C* svec, const double* pre, int f0, int fc,
+                    bool use_active = true) {
+    SysMap sm{dm.V, dm.R, d_run_of};
+    int tiles = 0;
+    VSAV_DISPATCH(FAM_PSI_COMB, {
+      long long nouter = fc;
+      ColArgs a = colargs(3, nouter, E_, NT_);
+      int L = 1 << a.logL;
+      int thr = std::max(a.TW, a.TW * L / E_);
+      size_t sm_b = (2 * (size_t)col_tile_elems(L, a.TW, ilog2(E_)) + (size_t)L * a.TW) * sizeof(C);
+      long long grid = (long long)a.tiles * fc;
+      tiles = a.tiles;
+      set_smem_attr<E_, NT_>((const void*)k_psi_cols_comb<T, E_, NT_>, sm_b);
+      prof.begin(st);
+      k_psi_cols_comb<T, E_, NT_><<<(unsigned)grid, thr, sm_b, st>>>(t1, t2, x, y, vb, svec, mode, d_adt, pre, ph.S4, a, sm,
+                                                                      use_active ? bupd : nullptr, f0, tab, part);
+      VSAV_COUNT_LAUNCH();
+      VSAV_LAUNCH_CHECK();
+      prof.end(st, KC_PSI_VEC, (double)fc * g.Pfull * 5.0 * sizeof(C));
+    })
+    return tiles;
+  }
+
   // time every variant of every pass family on scratch buffers; keep the fastest
   // process-wide tuning cache: handles of the same shape reuse the first choice
   static std::map<std::string, std::vector<int>>& tune_cache() { static std::map<std::string, std::vector<int>> m; return m; }
@@ -594,11 +639,11 @@ class Solver : public SolverBase {
   bool variant_ok(int fam, int v) const {
     int Lr = (fam == FAM_C2C || (fam == FAM_MUL && psi_full())) ? g.Nx : g.Nx / 2;
     int Lc = (g.nd == 3) ? std::min(g.Ny, g.Nz) : g.Ny;
-    int L = (fam == FAM_COLS || fam == FAM_COLS_PSI) ? Lc : Lr;
+    int L = (fam == FAM_COLS || fam == FAM_COLS_PSI || fam == FAM_PSI_INV2 || fam == FAM_PSI_COMB) ? Lc : Lr;
     return vE(v) <= L && vE(v) * VNT[v] / L >= 1;
   }
   void autotune() {
-    if (const char* forced = getenv("VSAV_TUNE")) {      // "c0,c1,c2,c3,c4,c5" (variant per family)
+    if (const char* forced = getenv("VSAV_TUNE")) {      // one digit per family: the variant index
       int k = 0;
       for (const char* q = forced; *q && k < FAM_N; ++q)
         if (*q >= '0' && *q <= '9') { int v = *q - '0'; if (v < NVAR && variant_ok(k, v)) choice[k] = v; ++k; }
@@ -623,9 +668,12 @@ class Solver : public SolverBase {
     bool was = prof.on;
     prof.on = false;
     bool have_mul = (g.nd == 2) && vt12 != nullptr;
+    // the fused x pass skips inactive systems: time it with every system active
+    if (have_mul) VSAV_CUDA(cudaMemsetAsync(bupd, 0xff, 3 * dm.R * sizeof(int), st));
     for (int fam = 0; fam < FAM_N; ++fam) {
       if (fam == FAM_MUL && !have_mul) continue;
-      if ((fam == FAM_C2C || fam == FAM_COLS_PSI) && !(g.nd == 2 && psi_full())) continue;
+      if ((fam == FAM_C2C || fam == FAM_COLS_PSI || fam == FAM_PSI_INV2 || fam == FAM_PSI_COMB) && !(g.nd == 2 && psi_full()))
+        continue;
       double best = 1e30;
       int bestv = 0;
       while (!variant_ok(fam, bestv) && bestv + 1 < NVAR) ++bestv;
@@ -639,6 +687,8 @@ class Solver : public SolverBase {
             case FAM_C2C: rows_c2c<false>(vb, nullptr, vt, 1.0, 3LL * V * g.Ny); break;
             case FAM_MUL: rows_mul(vt12, 2LL * psi_chunk() * g.Ny, psi_full(), 0, psi_chunk()); break;
             case FAM_COLS_PSI: cols(true, 3, 3LL * V, vb, nullptr, 1, 0, M_ONE, 1, vt, 1); break;
+            case FAM_PSI_INV2: psi_cols_inv2(vb, vt12, vt12 + 3LL * V * psi_n(), 0, 3 * V, false); break;
+            case FAM_PSI_COMB: psi_cols_comb(vt12, vt12 + 3LL * V * psi_n(), vb, vt, 0, nullptr, nullptr, 0, 3 * V, false); break;
             default: cols(false, g.nd == 2 ? 0 : 1, V, tmpH, nullptr, 1, 0, M_ONE, 1, tmpH, 1); break;
           }
         };
@@ -656,7 +706,7 @@ class Solver : public SolverBase {
     }
     prof.on = was;
     if (getenv("VSAV_VERBOSE")) {
-      const char* nm[FAM_N] = {"rows_r2c", "rows_c2r", "rows_c2c", "rows_mul", "cols", "cols_psi"};
+      const char* nm[FAM_N] = {"rows_r2c", "rows_c2r", "rows_c2c", "rows_mul", "cols", "cols_psi", "psi_inv2", "psi_comb"};
       for (int f = 0; f < FAM_N; ++f) for (int v = 0; v < NVAR; ++v) if (!variant_ok(f, v)) tune_ms[f][v] = -1;
       for (int f = 0; f < FAM_N; ++f) {
         fprintf(stderr, "[vsav autotune %s] %-9s", std::is_same<T, double>::value ? "fp64" : "fp32", nm[f]);
@@ -668,6 +718,7 @@ class Solver : public SolverBase {
     cudaEventDestroy(e1);
     // the scratch buffers carry garbage now: clear what later code expects zeroed
     VSAV_CUDA(cudaMemsetAsync(tmpH, 0, std::max<long long>(8 * dm.V, 9 * dm.R) * g.H * sizeof(C), st));
+    if (have_mul) VSAV_CUDA(cudaMemsetAsync(bupd, 0, 3 * dm.R * sizeof(int), st));
     VSAV_CUDA(cudaStreamSynchronize(st));
   }
 
@@ -1003,6 +1054,8 @@ class Solver : public SolverBase {
 
   // y = P^-1 A in (+ dots), chunk by chunk: y-inverse (2 multipliers), fused
   // x pass (inverse, x M_psi, forward), y-forward, combine
+  EW dot_ew{};                 // partial layout of the dots of the last matvec
+  bool fused_ops = true;       // FULL form: fused column passes (VSAV_PSI_FUSED=0: separate kernels)
   void matvec(const C* in, C* out, int mode, const C* svec, bool precond = true) {
     const int V = dm.V;
     const long long F = 3LL * V, n = psi_n();
@@ -1013,10 +1066,19 @@ class Solver : public SolverBase {
     VGeom vg{full ? 1 : 0, g.Nx, g.Ny, g.kp, g.nkx, ilog2(g.Nx), n, g.kxs, g.kys};
     SysMap sm{V, dm.R, d_run_of};
     const double* pre = precond ? mmax_r : nullptr;
+    dot_ew = e;
     for (int f0 = 0; f0 < F; f0 += Fc) {
       const int fc = (int)std::min<long long>(Fc, F - f0);
       C* t1 = vt12;
       C* t2 = vt12 + (long long)fc * n;
+      if (full && fused_ops) {
+        // one read of x for both inverse passes; the forward pass carries the combine
+        psi_cols_inv2(in, t1, t2, f0, fc);
+        rows_mul(t1, 2LL * fc * g.Ny, full, f0, fc);
+        const int tiles = psi_cols_comb(t1, t2, in, out, mode, svec, pre, f0, fc);
+        dot_ew.bpf = tiles;
+        continue;
+      }
       cols(true, geo, fc, in + f0 * n, nullptr, 1, 0, full ? M_DX0 : M_DXZ, ph.S4, t1, 1);
       cols(true, geo, fc, in + f0 * n, nullptr, 1, 0, M_DY, ph.S4, t2, 1);
       rows_mul(t1, 2LL * fc * g.Ny, full, f0, fc);
@@ -1142,12 +1204,12 @@ class Solver : public SolverBase {
     if (hv_cap) { hv_count = 0; harvest_snap(x, vr); }
     krylov_loop(itmax, [&]() {
       matvec(vp, vv, 0, nullptr);                       // v = M^-1 A p ; <c, v>
-      fin(4, (int)F, e, fd);
+      fin(4, (int)F, dot_ew, fd);
       k_bi_alpha<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, sm, S, (int)F); VSAV_COUNT_LAUNCH();
       k_psi_s<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(vr, vv, vs, bst, sm, e); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
       matvec(vs, vt, 1, vs);                            // t = M^-1 A s ; <t,s>, <t,t>
-      fin(4, (int)F, e, fd);
+      fin(4, (int)F, dot_ew, fd);
       k_bi_omega<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, sm, S, (int)F); VSAV_COUNT_LAUNCH();
       k_psi_update<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(x, vr, vp, vs, vt, vb, bst, vg, sm, e, part); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
@@ -1190,13 +1252,13 @@ class Solver : public SolverBase {
     krylov_loop(itmax, [&]() {
       precond_apply(vp, vph);
       matvec(vph, vv, 0, nullptr, false);               // v = A p^ ; <c, v>
-      fin(4, (int)F, e, fd);
+      fin(4, (int)F, dot_ew, fd);
       k_bi_alpha<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, sm, S, (int)F); VSAV_COUNT_LAUNCH();
       k_psi_s<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(vr, vv, vs, bst, sm, e); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
       precond_apply(vs, vsh);
       matvec(vsh, vt, 1, vs, false);                    // t = A s^ ; <t, s>, <t, t>
-      fin(4, (int)F, e, fd);
+      fin(4, (int)F, dot_ew, fd);
       k_bi_omega<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, sm, S, (int)F); VSAV_COUNT_LAUNCH();
       k_psi_update<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(x, vr, vph, vs, vt, vb, bst, vg, sm, e, part, vsh); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
