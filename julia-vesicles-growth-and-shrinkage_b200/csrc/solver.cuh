@@ -29,8 +29,8 @@ struct Options {
   double psi_rtol = 1e-12, psi_atol = 1e-14;
   int check_every_iter = 1;  // read back convergence flags each BiCGSTAB iteration
   int psi_mixed = 0;         // FP64 fields with the psi BiCGSTAB in FP32 + FP64 iterative refinement
-  int psi_refine = 2;        // refinement sweeps of the mixed mode
-  double psi_inner_rtol = 1e-6;
+  int psi_refine_min = 1;    // least refinement sweeps of the mixed mode
+  double psi_inner_rtol = 1e-6;   // tightest relative tolerance of one FP32 sweep
   int graph = 1;             // vsav_run replays each time step as a CUDA graph
 };
 
@@ -1526,7 +1526,8 @@ class Solver : public SolverBase {
 
 // Mixed precision (FP64 fields): b (FP64, full spectrum) -> x by sweeps of
 //   r = b - A x (FP64 operator, no preconditioner);  A d = r solved by the
-//   FP32 helper's BiCGSTAB to psi_inner_rtol;  x += d.
+//   FP32 helper's BiCGSTAB;  x += d, over enough sweeps that the product of the
+//   sweeps' relative tolerances (each >= psi_inner_rtol) reaches psi_rtol.
 // The FP32 solve does most of the work; the FP64 residual keeps the result at
 // FP64 accuracy after a few sweeps (classical iterative refinement).
 template <typename T>
@@ -1543,7 +1544,13 @@ void Solver<T>::psi_solve_mixed() {
     C* x = psi_x();
     VSAV_CUDA(cudaMemsetAsync(x, 0, nc * sizeof(C), st));
     VSAV_CUDA(cudaMemsetAsync(bupd, 0xff, 3 * R * sizeof(int), st));     // every system active in A x
-    for (int ref = 0; ref < std::max(1, opt.psi_refine); ++ref) {
+    // the requested relative tolerance is split over the sweeps, each FP32 solve
+    // reaching at most 1e-6 (rtol 1e-12: two sweeps at 1e-6; 1e-8: two at 1e-4)
+    const double rt = std::min(std::max(opt.psi_rtol, 1e-15), 0.5);
+    const int nsw = std::max(std::max(1, (int)std::ceil(std::log(rt) / std::log(opt.psi_inner_rtol) - 1e-9)),
+                             opt.psi_refine_min);
+    const double inner = std::pow(rt, 1.0 / nsw);
+    for (int ref = 0; ref < nsw; ++ref) {
       const C* r = vb;
       if (ref > 0) {
         VSAV_CUDA(cudaMemsetAsync(bupd, 0xff, 3 * R * sizeof(int), st));
@@ -1552,7 +1559,7 @@ void Solver<T>::psi_solve_mixed() {
         r = vs;
       }
       k_cast<double2, float2><<<gridfor(nc), 256, 0, st>>>(r, H->vb, nc); VSAV_COUNT_LAUNCH();
-      H->psi_krylov(H->psi_x(), opt.psi_inner_rtol, opt.psi_itmax);
+      H->psi_krylov(H->psi_x(), inner, opt.psi_itmax);
       k_add_cast<float2, double2><<<gridfor(nc), 256, 0, st>>>(H->psi_x(), x, nc); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
     }
