@@ -292,6 +292,8 @@ class Solver : public SolverBase {
       : ph(p), opt(o), dm(d) {
     VSAV_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     if (const char* env = getenv("VSAV_PSI_FUSED")) fused_ops = atoi(env) != 0;
+    // VSAV_GRAPH=0 runs every step eagerly (kernel-level profilers see each launch)
+    if (const char* env = getenv("VSAV_GRAPH")) if (atoi(env) == 0) opt.graph = 0;
     g.nd = d.nd; g.Nx = d.Nx; g.Ny = d.Ny; g.Nz = (d.nd == 3) ? d.Nz : 1;
     g.nkx = d.Nx / 2 + 1;
     g.kp = (g.nkx + 15) / 16 * 16;
