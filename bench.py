@@ -131,14 +131,21 @@ def dist_init():
     return ws, rank, local
 
 
-def max_over_ranks(x, ws):
+def max_over_ranks(x, ws, device="cuda"):
     if ws == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def aggregate(steps, ms, ws, device="cuda"):
+    """Whole-job rate of ws replicas that each timed `steps` steps in `ms` ms of
+    device time: all replicas' steps over the slowest replica's time."""
+    ms_max = max_over_ranks(ms, ws, device)
+    return ws * steps / (ms_max / 1000.0), ms_max
 
 
 def barrier(ws):
@@ -238,8 +245,7 @@ def run_ours(args):
     n += args.steps
     clocks = clk.stop()
     barrier(ws)
-    ms_max = max_over_ranks(ms, ws)
-    value = ws * args.steps / (ms_max / 1000.0)
+    value, ms_max = aggregate(args.steps, ms, ws)
     iters = h.psi_stats()[:, 0].tolist()
     if args.quick:
         if rank == 0:

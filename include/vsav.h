@@ -106,6 +106,7 @@ int vsav_set_scalars(vsav_handle* h, int32_t level, const double* q4);
 int vsav_get_scalars(vsav_handle* h, int32_t level, double* q4);
 /* present.dt per run (simulation.jl:73) */
 int vsav_set_dt(vsav_handle* h, const double* dt);
+int vsav_get_dt(vsav_handle* h, double* dt);
 /* present.A0 per vesicle field */
 int vsav_set_A0(vsav_handle* h, const double* A0);
 int vsav_get_A0(vsav_handle* h, double* A0);

@@ -46,18 +46,25 @@ def up_to_date(path, inputs=None):
 
 def _compile(unit, verbose):
     obj = os.path.join(OBJ, unit.replace(".cu", ".o"))
-    if up_to_date(obj, deps(os.path.join(SRC, unit))):
+    inputs = deps(os.path.join(SRC, unit))
+    if up_to_date(obj, inputs):
         return obj
+    # stamp the object with its inputs' newest time at the start, so that a source
+    # edited while this compiles still counts as newer
+    stamp = max(os.path.getmtime(s) for s in inputs)
     cmd = [NVCC] + FLAGS + ["-c", "-o", obj + ".tmp", os.path.join(SRC, unit)]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)
     os.replace(obj + ".tmp", obj)
+    os.utime(obj, (stamp, stamp))
     return obj
 
 
 def build(force=False, verbose=True):
-    if not force and up_to_date(OUT):
+    objs = [os.path.join(OBJ, u.replace(".cu", ".o")) for u in UNITS]
+    if not force and all(up_to_date(o, deps(os.path.join(SRC, u))) for o, u in zip(objs, UNITS)) \
+            and os.path.exists(OUT) and all(os.path.getmtime(o) <= os.path.getmtime(OUT) for o in objs):
         return OUT
     os.makedirs(OBJ, exist_ok=True)
     if force:

@@ -261,13 +261,25 @@ __global__ void __launch_bounds__(NT, MinB<E, NT>::v) k_psi_cols_inv2(const cplx
   const ColLay lay{a.TW, Log2<E>::v};
   C* const buf[2] = {s, s + col_tile_elems(L, a.TW, Log2<E>::v)};
   const C* xin = x + (long long)f * a.O + c;
+  // small E: the raw tile stays in registers for the second direction
+  constexpr int EK = E <= 8 ? E : 1;
+  C xr[EK];
+  if constexpr (E <= 8) {
+#pragma unroll
+    for (int j = 0; j < E; ++j) xr[j] = valid ? xin[(long long)(i + j * LE) * a.S] : mk<C>(0.0, 0.0);
+  }
 #pragma unroll 1
   for (int d = 0; d < 2; ++d) {
     const int mult = d == 0 ? M_DX0 : M_DY;
     C v[E];
     if (valid) {
 #pragma unroll
-      for (int j = 0; j < E; ++j) v[j] = xin[(long long)(i + j * LE) * a.S] * col_mult<C>(a, mult, S4, c, i + j * LE, 0);
+      for (int j = 0; j < E; ++j) {
+        C xv;
+        if constexpr (E <= 8) xv = xr[j];
+        else xv = xin[(long long)(i + j * LE) * a.S];
+        v[j] = xv * col_mult<C>(a, mult, S4, c, i + j * LE, 0);
+      }
     } else {
 #pragma unroll
       for (int j = 0; j < E; ++j) v[j] = mk<C>(0.0, 0.0);

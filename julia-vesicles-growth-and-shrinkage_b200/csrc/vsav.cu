@@ -178,6 +178,9 @@ int vsav_set_dt(vsav_handle* h, const double* dt) {
     return VSAV_OK;
   });
 }
+int vsav_get_dt(vsav_handle* h, double* dt) {
+  return guard(h, [&] { if (!dt) throw std::runtime_error("dt is NULL"); h->s->get_dt(dt); return VSAV_OK; });
+}
 int vsav_set_A0(vsav_handle* h, const double* a0) {
   return guard(h, [&] { if (!a0) throw std::runtime_error("bad args"); h->s->set_A0(a0); return VSAV_OK; });
 }

@@ -157,6 +157,11 @@ class Handle:
         a = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, float), (self.R,)), dtype=np.float64)
         self._chk(self.lib.vsav_set_dt(self.h, L.dptr(a)))
 
+    def get_dt(self):
+        a = np.empty(self.R)
+        self._chk(self.lib.vsav_get_dt(self.h, L.dptr(a)))
+        return a
+
     def set_A0(self, a0):
         a = np.ascontiguousarray(np.asarray(a0, dtype=np.float64).reshape(self.V))
         self._chk(self.lib.vsav_set_A0(self.h, L.dptr(a)))
