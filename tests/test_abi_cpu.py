@@ -81,3 +81,30 @@ def test_workloads_are_seeded():
     assert phi.shape == (3, 64, 64) and np.all(np.abs(phi) <= 1)
     # vesicles do not overlap: at most one field is inside (phi > 0) at each point
     assert np.max(np.sum(phi > 0, axis=0)) <= 1
+
+
+def test_net_and_psi_entry_points_reject_bad_arguments():
+    """The learned-preconditioner and harvest entry points validate their
+    arguments and report errors (no device needed for these paths)."""
+    import ctypes as ct
+    from vsav import _lib
+    lib = _lib.load()
+    assert lib.vsav_net_nparams() == 7409
+    out = ct.c_void_p()
+    assert lib.vsav_net_create(0, 0, ct.byref(out)) == -1          # empty capacity
+    assert lib.vsav_net_destroy(None) == -1
+    th = np.zeros(7409)
+    assert lib.vsav_net_set_params(None, _lib.dptr(th)) == -1
+    assert lib.vsav_set_psi_net(None, _lib.dptr(th)) == -1
+    assert lib.vsav_psi_harvest(None, 4) == -1
+    assert lib.vsav_get_dt(None, _lib.dptr(th)) == -1
+
+
+@pytest.mark.skipif(cuda_available(), reason="needs a machine without a CUDA device")
+def test_net_create_fails_loudly_without_gpu():
+    import ctypes as ct
+    from vsav import _lib
+    lib = _lib.load()
+    out = ct.c_void_p()
+    assert lib.vsav_net_create(1024, 0, ct.byref(out)) == -2       # VSAV_E_CUDA
+    assert b"CUDA" in lib.vsav_net_last_error(None)
