@@ -116,6 +116,23 @@ int vsav_get_A0(vsav_handle* h, double* A0);
  * mu/nu, old = deepcopy(present). */
 int vsav_init_state(vsav_handle* h, int32_t hats_given);
 
+/* Seeded shape initial conditions computed on the device (2D; no counterpart in
+ * the reference, whose generate_initial_condition builds hard-coded shapes on
+ * the host, Init.jl:74-216): one shape per vesicle field (V), boundary radius
+ * R(theta) = a b / sqrt((b cos theta)^2 + (a sin theta)^2)
+ *            + sum_k amp[k] cos(m[k] theta + phase[k])
+ * in the frame rotated by rot about (cx, cy) on the grid x_i = -Lx/2 + Lx i/Nx,
+ * phi = tanh((R - r) / (sqrt(2) epsilon)) (Init.jl:113),
+ * psi = psi_in (1 + phi)/2 + psi_out (1 - phi)/2, u = p = 0; then
+ * vsav_init_state(h, 0). */
+typedef struct vsav_shape2d {
+  double cx, cy, a, b, rot, psi_in, psi_out;
+  int32_t nmodes;               /* 0..8 */
+  int32_t m[8];
+  double amp[8], phase[8];
+} vsav_shape2d;
+int vsav_init_shapes2d(vsav_handle* h, const vsav_shape2d* shapes);
+
 /* solve_step1..7 (Solvers.jl:14,144,242,267,344,431,459); n is the step index
  * of simulation.jl:71 (n == 1 -> BDF1, else BDF2).  Results stay on the device
  * (Step1Cache and the step intermediates); read them with vsav_get_work. */

@@ -54,6 +54,8 @@ class SolverBase {
   virtual void set_A0(const double* a0) = 0;
   virtual void get_A0(double* a0) = 0;
   virtual void init_state(int hats_given) = 0;
+  // seeded-shape initial phi/psi on the device (2D), u = p = 0, then init_state
+  virtual void init_shapes2d(const struct Shape2D* shapes) = 0;
   virtual void step1(int n) = 0;
   virtual void step2(int n) = 0;
   virtual void step3() = 0;
@@ -216,6 +218,39 @@ __global__ void k_sub(const T* __restrict__ b, const T* __restrict__ y, T* __res
 }
 
 template <typename T> class Solver;
+
+// A 2D vesicle shape: boundary radius R(theta) = a b / sqrt((b cos)^2 + (a sin)^2)
+// + sum_k amp_k cos(m_k theta + phase_k) in the frame rotated by rot about
+// (cx, cy); phi = tanh((R - r) / (sqrt(2) eps)), psi = psi_in (1+phi)/2 + psi_out (1-phi)/2
+// (the tanh profile of Init.jl:113).
+struct Shape2D {
+  double cx, cy, a, b, rot, psi_in, psi_out;
+  int nmodes;
+  int m[8];
+  double amp[8], phase[8];
+};
+
+template <typename T>
+__global__ void k_shapes2d(T* __restrict__ phi, T* __restrict__ psi, const Shape2D* __restrict__ sh, int V, int Nx, int Ny,
+                           double Lx, double Ly, double eps) {
+  const long long P = (long long)Nx * Ny, tot = (long long)V * P;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < tot; k += (long long)gridDim.x * blockDim.x) {
+    const int v = (int)(k / P);
+    const long long q = k - (long long)v * P;
+    const int j = (int)(q / Nx), i = (int)(q - (long long)j * Nx);
+    const Shape2D s = sh[v];
+    const double x = -0.5 * Lx + Lx * i / Nx - s.cx, y = -0.5 * Ly + Ly * j / Ny - s.cy;
+    const double cr = cos(s.rot), sr = sin(s.rot);
+    const double xr = cr * x + sr * y, yr = -sr * x + cr * y;
+    const double th = atan2(yr, xr), r = hypot(xr, yr);
+    const double bc = s.b * cos(th), as = s.a * sin(th);
+    double R = s.a * s.b / sqrt(bc * bc + as * as);
+    for (int k2 = 0; k2 < s.nmodes; ++k2) R += s.amp[k2] * cos(s.m[k2] * th + s.phase[k2]);
+    const double p = tanh((R - r) / (1.4142135623730951 * eps));
+    phi[k] = (T)p;
+    psi[k] = (T)(s.psi_in * (1 + p) / 2 + s.psi_out * (1 - p) / 2);
+  }
+}
 
 // Book-keeping of one step-graph capture: the kernels captured outside the
 // Krylov loops, and per loop (a WHILE node) the kernels of its body and the
@@ -1013,6 +1048,21 @@ class Solver : public SolverBase {
   }
 
   // simulation.jl:22-53
+  void init_shapes2d(const Shape2D* shapes) override {
+    if (g.nd != 2) throw std::runtime_error("shape initial conditions are 2D");
+    const int V = dm.V, R = dm.R;
+    const long long VP = (long long)V * g.P;
+    for (int v = 0; v < V; ++v)
+      if (shapes[v].nmodes < 0 || shapes[v].nmodes > 8 || !(shapes[v].a > 0) || !(shapes[v].b > 0))
+        throw std::runtime_error("bad shape " + std::to_string(v) + ": need a, b > 0 and 0..8 modes");
+    VSAV_CUDA(cudaMemcpyAsync(stage, shapes, V * sizeof(Shape2D), cudaMemcpyHostToDevice, st));
+    k_shapes2d<T><<<gridfor(VP), 256, 0, st>>>(phys4[0], phys4[0] + VP, reinterpret_cast<const Shape2D*>(stage), V, g.Nx,
+                                               g.Ny, dm.Lx, dm.Ly, ph.eps); VSAV_COUNT_LAUNCH();
+    VSAV_LAUNCH_CHECK();
+    VSAV_CUDA(cudaMemsetAsync(uphys[0], 0, (g.nd + 1) * (long long)R * g.P * sizeof(T), st));
+    init_state(0);
+  }
+
   void init_state(int hats_given) override {
     const int V = dm.V, R = dm.R;
     const long long VP = (long long)V * g.P, VH = (long long)V * g.H;

@@ -187,6 +187,16 @@ int vsav_set_A0(vsav_handle* h, const double* a0) {
 int vsav_get_A0(vsav_handle* h, double* a0) {
   return guard(h, [&] { if (!a0) throw std::runtime_error("bad args"); h->s->get_A0(a0); return VSAV_OK; });
 }
+int vsav_init_shapes2d(vsav_handle* h, const vsav_shape2d* shapes) {
+  return guard(h, [&] {
+    if (!shapes) throw std::runtime_error("shapes is NULL");
+    static_assert(sizeof(vsav_shape2d) == sizeof(Shape2D), "shape struct layouts differ");
+    std::vector<Shape2D> s(h->V);
+    std::memcpy(s.data(), shapes, h->V * sizeof(Shape2D));
+    h->s->init_shapes2d(s.data());
+    return check_status(h, nullptr) < 0 ? VSAV_E_WC_NEGATIVE : VSAV_OK;
+  });
+}
 int vsav_init_state(vsav_handle* h, int32_t hats_given) {
   return guard(h, [&] { h->s->init_state(hats_given); return check_status(h, nullptr) < 0 ? VSAV_E_WC_NEGATIVE : VSAV_OK; });
 }

@@ -171,6 +171,25 @@ class Handle:
         self._chk(self.lib.vsav_get_A0(self.h, L.dptr(a)))
         return a
 
+    def init_shapes(self, shapes):
+        """Initial state from seeded shape parameters, evaluated on the device
+        (2D): one dict per vesicle field with cx, cy, a, b, rot, psi_in, psi_out
+        and modes [(m, amp, phase), ...] (at most 8); u = p = 0; then init_state."""
+        if len(shapes) != self.V:
+            raise ValueError(f"need {self.V} shapes, got {len(shapes)}")
+        arr = (L.VsavShape2D * self.V)()
+        for k, sh in enumerate(shapes):
+            s = arr[k]
+            for f in ("cx", "cy", "a", "b", "rot", "psi_in", "psi_out"):
+                setattr(s, f, float(sh[f]))
+            modes = list(sh.get("modes", []))
+            if len(modes) > 8:
+                raise ValueError("at most 8 modes per shape")
+            s.nmodes = len(modes)
+            for j, (m, amp, ph) in enumerate(modes):
+                s.m[j], s.amp[j], s.phase[j] = int(m), float(amp), float(ph)
+        self._chk(self.lib.vsav_init_shapes2d(self.h, arr))
+
     def init_state(self, phi, psi, u=None, p=None):
         """generate_initial_condition's FFTs (Init.jl:199-216) + simulation.jl:22-53."""
         self.set_field("phi", phi)

@@ -55,6 +55,14 @@ def _blend(phi, pin, pout):
     return pin * (1 + phi) / 2 + pout * (1 - phi) / 2
 
 
+def single2d_shape(seed: int = 0, a: float = 1.2, b: float = 0.8, amp: float = 0.02, psi_inside: float = 0.6,
+                   psi_outside: float = 0.2):
+    """The single2d shape as parameters (for the device generator, vsav_init_shapes2d)."""
+    rng = np.random.default_rng(seed)
+    modes = [(m, amp, rng.uniform(0, 2 * np.pi)) for m in range(2, 7)]
+    return dict(cx=0.0, cy=0.0, a=a, b=b, rot=0.0, psi_in=psi_inside, psi_out=psi_outside, modes=modes)
+
+
 def single2d(n: int = 128, eps: float = 0.08, seed: int = 0, a: float = 1.2, b: float = 0.8,
              amp: float = 0.02, psi_inside: float = 0.6, psi_outside: float = 0.2):
     """phi, psi arrays [1][n][n]."""
@@ -71,13 +79,18 @@ def single2d(n: int = 128, eps: float = 0.08, seed: int = 0, a: float = 1.2, b: 
     return phi, psi
 
 
-def multi2d(n: int, N: int, eps: float, seed: int, psi_lo: float = 0.4, psi_hi: float = 0.8,
-            psi_outside: float = 0.2, L: float = 2 * math.pi, max_tries: int = 20000):
-    """N non-overlapping seeded ellipses.  Returns phi, psi [N][n][n] and the
-    per-vesicle inside psi values."""
+def multi2d_shapes(N: int, eps: float, seed: int, psi_lo: float = 0.4, psi_hi: float = 0.8,
+                   psi_outside: float = 0.2, L: float = 2 * math.pi, max_tries: int = 20000):
+    """The multi2d shapes as parameters (same seeded draws as multi2d)."""
     rng = np.random.default_rng(seed)
-    x = grid(n, L)
-    X, Y = np.meshgrid(x, x, indexing="xy")
+    shapes = _place(rng, N, eps, L, max_tries)
+    pin = rng.uniform(psi_lo, psi_hi, size=N)
+    return [dict(cx=cx, cy=cy, a=rad, b=rad * ratio, rot=rot, psi_in=float(pin[k]), psi_out=psi_outside, modes=[])
+            for k, (cx, cy, rad, ratio, rot) in enumerate(shapes)]
+
+
+def _place(rng, N, eps, L, max_tries):
+    """Rejection-sampled non-overlapping ellipse parameters (cx, cy, rad, ratio, rot)."""
     shapes = []
     tries = 0
     while len(shapes) < N:
@@ -92,6 +105,17 @@ def multi2d(n: int, N: int, eps: float, seed: int, psi_lo: float = 0.4, psi_hi: 
         ok = all(math.hypot(cx - s[0], cy - s[1]) >= rad + s[2] + 4 * eps for s in shapes)
         if ok:
             shapes.append((cx, cy, rad, ratio, rot))
+    return shapes
+
+
+def multi2d(n: int, N: int, eps: float, seed: int, psi_lo: float = 0.4, psi_hi: float = 0.8,
+            psi_outside: float = 0.2, L: float = 2 * math.pi, max_tries: int = 20000):
+    """N non-overlapping seeded ellipses.  Returns phi, psi [N][n][n] and the
+    per-vesicle inside psi values."""
+    rng = np.random.default_rng(seed)
+    x = grid(n, L)
+    X, Y = np.meshgrid(x, x, indexing="xy")
+    shapes = _place(rng, N, eps, L, max_tries)
     phi = np.empty((N, n, n))
     psi = np.empty((N, n, n))
     pin = rng.uniform(psi_lo, psi_hi, size=N)
@@ -161,6 +185,16 @@ def ensemble(n_runs: int = 64, n: int = 256, eps: float = 0.08, seed: int = 0, n
         tin += [0.65 if k % 2 == 0 else 0.1 for k in range(N)]
     kw = params(eps, max(sizes), tin, [0.8] * len(tin), dt, 100 * dt, n, n)
     return kw, sizes, np.concatenate(phis), np.concatenate(psis)
+
+
+def ensemble_shapes(n_runs: int = 64, eps: float = 0.08, seed: int = 0, nmin: int = 1, nmax: int = 4):
+    """The shapes of ensemble() as parameters, run after run (device generator)."""
+    rng = np.random.default_rng(seed)
+    sizes = [int(k) for k in rng.integers(nmin, nmax + 1, size=n_runs)]
+    out = []
+    for r, N in enumerate(sizes):
+        out += multi2d_shapes(N, eps, seed * 1000 + r, 0.3, 0.9)
+    return sizes, out
 
 
 # ---------------------------------------------------------------------------

@@ -38,7 +38,7 @@ def test_struct_layouts_match_header():
     from vsav import _lib
     txt = open(HEADER).read()
     for cname, py in (("vsav_config", _lib.VsavConfig), ("vsav_options", _lib.VsavOptions),
-                      ("vsav_status", _lib.VsavStatus)):
+                      ("vsav_status", _lib.VsavStatus), ("vsav_shape2d", _lib.VsavShape2D)):
         body = re.search(r"typedef struct %s \{(.*?)\} %s;" % (cname, cname), txt, re.S).group(1)
         body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
         names = []
@@ -47,7 +47,7 @@ def test_struct_layouts_match_header():
             if not decl:
                 continue
             decl = re.sub(r"^(const\s+)?\w+\s*\**\s*", "", decl)
-            names += [x.strip().lstrip("*") for x in decl.split(",")]
+            names += [re.sub(r"\[\d+\]$", "", x.strip().lstrip("*")) for x in decl.split(",")]
         assert names == [f[0] for f in py._fields_], cname
 
 

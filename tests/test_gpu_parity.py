@@ -151,23 +151,50 @@ def test_fp64_step_intermediates():
     h.close()
 
 
-def test_ensemble_runs_are_independent():
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_ensemble_runs_are_independent(prec):
     """R runs of different vesicle counts in one handle advance exactly like
-    separate handles (per-run SAV scalars, velocity and psi systems)."""
+    separate handles (per-run SAV scalars, velocity and psi systems), also
+    with the mixed-precision solve and graph-replayed steps."""
     from vsav import ics
     kwa, phia, psia, _ = ics.workload("multi2d_512x4", seed=1, n_override=64, N_override=1, eps_override=0.2)
     kwb, phib, psib, _ = ics.workload("multi2d_512x4", seed=2, n_override=64, N_override=2, eps_override=0.2)
     for kw in (kwa, kwb):
         kw["dt"] = 1e-6
     kwe = dict(kwa, N=1, psi_in_v=kwa["psi_in_v"] + kwb["psi_in_v"], psi_out_v=kwa["psi_out_v"] + kwb["psi_out_v"])
-    he = make(kwe, run_sizes=[1, 2])
+    he = make(kwe, run_sizes=[1, 2], precision=prec)
     he.init_state(np.concatenate([phia, phib]), np.concatenate([psia, psib]))
     Ee, _ = he.run(1, 3, monitor=True)
     for r, (kw, phi, psi, sl) in enumerate(((kwa, phia, psia, slice(0, 1)), (kwb, phib, psib, slice(1, 3)))):
-        h = make(kw)
+        h = make(kw, precision=prec)
         h.init_state(phi, psi)
         E, _ = h.run(1, 3, monitor=True)
         assert rel(he.get_field("phi")[sl], h.get_field("phi")) < 1e-12
+        assert rel(he.get_field("u")[r], h.get_field("u")[0]) < 1e-12
+        np.testing.assert_allclose(he.get_scalars()[r], h.get_scalars()[0], rtol=1e-12)
+        np.testing.assert_allclose(Ee[:, r], E[:, 0], rtol=1e-12)
+        h.close()
+    he.close()
+
+
+def test_ensemble_3d_runs_are_independent():
+    """Two 3D runs (one vesicle each, the reference's 3D coupling) in one handle
+    advance like two separate handles."""
+    from vsav import ics
+    runs = [ics.workload("single3d_128", seed=s, n_override=32) for s in (1, 2)]
+    for kw, *_ in runs:
+        kw["dt"] = 1e-5
+    kwa = runs[0][0]
+    kwe = dict(kwa, N=1, psi_in_v=kwa["psi_in_v"] + runs[1][0]["psi_in_v"],
+               psi_out_v=kwa["psi_out_v"] + runs[1][0]["psi_out_v"])
+    he = make(kwe, run_sizes=[1, 1])
+    he.init_state(np.concatenate([runs[0][1], runs[1][1]]), np.concatenate([runs[0][2], runs[1][2]]))
+    Ee, _ = he.run(1, 3, monitor=True)
+    for r, (kw, phi, psi, _) in enumerate(runs):
+        h = make(kw)
+        h.init_state(phi, psi)
+        E, _ = h.run(1, 3, monitor=True)
+        assert rel(he.get_field("phi")[r:r + 1], h.get_field("phi")) < 1e-12
         assert rel(he.get_field("u")[r], h.get_field("u")[0]) < 1e-12
         np.testing.assert_allclose(he.get_scalars()[r], h.get_scalars()[0], rtol=1e-12)
         np.testing.assert_allclose(Ee[:, r], E[:, 0], rtol=1e-12)
@@ -356,3 +383,34 @@ def test_full_size_1024x8_properties():
     assert np.all(np.diff(Em[:, 0]) <= 0) and np.all(np.diff(E64[:, 0]) <= 0)
     assert np.max(np.abs(Em - E64) / np.abs(E64)) < 1e-5
     hm.close()
+
+
+@pytest.mark.parametrize("which", ["single2d", "multi2d", "ensemble"])
+def test_device_shapes_match_host_generator(which):
+    """vsav_init_shapes2d evaluates the seeded shapes on the device: the same
+    phi/psi (and so the same state after two steps) as the host generator."""
+    from vsav import ics
+    run_sizes = None
+    if which == "single2d":
+        kw, phi, psi, _ = ics.workload("single2d_128", n_override=64)
+        shapes = [ics.single2d_shape(seed=0)]
+    elif which == "multi2d":
+        kw, phi, psi, _ = ics.workload("multi2d_512x4", seed=3, n_override=128, N_override=3, eps_override=0.1)
+        shapes = ics.multi2d_shapes(3, 0.1, 3)
+    else:
+        kw, run_sizes, phi, psi = ics.ensemble(n_runs=4, n=64, eps=0.2)
+        sizes, shapes = ics.ensemble_shapes(n_runs=4, eps=0.2)
+        assert sizes == run_sizes
+    kw["dt"] = 1e-6
+    hd = make(kw, run_sizes=run_sizes)
+    hd.init_shapes(shapes)
+    hh = make(kw, run_sizes=run_sizes)
+    hh.init_state(phi, psi)
+    for k in ("phi", "psi", "mu", "nu"):
+        assert rel(hd.get_field(k), hh.get_field(k)) < 1e-12, k
+    hd.run(1, 2)
+    hh.run(1, 2)
+    for k in FIELDS:
+        assert rel(hd.get_field(k), hh.get_field(k)) < 1e-10, k
+    hd.close()
+    hh.close()
