@@ -116,6 +116,22 @@ int vsav_get_A0(vsav_handle* h, double* A0);
  * mu/nu, old = deepcopy(present). */
 int vsav_init_state(vsav_handle* h, int32_t hats_given);
 
+/* generate_initial_condition(conf, ops, state_type) (Init.jl:74-216,
+ * Init_3d.jl:67-152) evaluated on the device, then vsav_init_state(h, 0) (the
+ * rest of simulation.jl:22-53).  goal: 'g' or 's' (Config.goal).  Every run of
+ * the handle gets the shapes of its own N: 2D state_type 1 ellipse, 2 smoothed
+ * triangle, 3 star, 4 random blob (N = 1), 7/8 stars (N = 2, 3); 3D state_type 1
+ * ellipsoid (N = 1); the other types the reference accepts leave phi = 0.
+ * psi = -0.1 phi + 0.7 (goal s) or -0.35 phi + 0.45.  blob_u: [R][20], the
+ * uniform draws of state_type 4 in the reference's order (an, pn for k = 1..10;
+ * Init.jl:155-159), NULL otherwise.  The reference's error() cases (a state_type
+ * invalid for N, a goal that contradicts state_type 7/8, N = 2 with a goal other
+ * than g/s) return VSAV_E_INVALID, and so do the cases where it raises UndefVarError
+ * (N > 3; 3D state_type 7). */
+#define VSAV_GOAL_G 'g'
+#define VSAV_GOAL_S 's'
+int vsav_generate_initial_condition(vsav_handle* h, int32_t state_type, int32_t goal, const double* blob_u);
+
 /* Seeded shape initial conditions computed on the device (2D; no counterpart in
  * the reference, whose generate_initial_condition builds hard-coded shapes on
  * the host, Init.jl:74-216): one shape per vesicle field (V), boundary radius

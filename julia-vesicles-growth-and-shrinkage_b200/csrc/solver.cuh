@@ -7,6 +7,8 @@
 // (src/Types.jl:243-265) achieves by copying.
 #pragma once
 #include <vector>
+#include <cstring>
+#include <string>
 #include <memory>
 #include <algorithm>
 #include <type_traits>
@@ -56,6 +58,7 @@ class SolverBase {
   virtual void init_state(int hats_given) = 0;
   // seeded-shape initial phi/psi on the device (2D), u = p = 0, then init_state
   virtual void init_shapes2d(const struct Shape2D* shapes) = 0;
+  virtual void init_reference_shapes(int state_type, int goal, const double* blob_u) = 0;
   virtual void step1(int n) = 0;
   virtual void step2(int n) = 0;
   virtual void step3() = 0;
@@ -252,6 +255,73 @@ __global__ void k_shapes2d(T* __restrict__ phi, T* __restrict__ psi, const Shape
   }
 }
 
+// One vesicle field of the reference's generate_initial_condition (Init.jl:74-197,
+// Init_3d.jl:67-137), resolved on the host from (state_type, goal, N of the run):
+// the shape kind, its centre and constants, psi = alpha phi + beta (Init.jl:191-197).
+enum { RS_ZERO = 0, RS_ELLIPSE, RS_TRIANGLE, RS_STAR, RS_BLOB, RS_ELLIPSOID };
+struct RefShape {
+  int kind;
+  double cx, cy, cz;
+  double R0, amp;                    // ELLIPSE/ELLIPSOID: R; TRIANGLE: radius; STAR/BLOB: R0, amplitude
+  double alpha, beta;
+  double an[10], pn[10];             // BLOB: R(theta) = R0 + sum_k an_k R0 cos(k theta + pn_k)
+};
+
+// The grid is x_i = i dx from 0 (range(0, Lx - dx, length=Nx), Init.jl:80-83);
+// angles are Julia's atan(X - cx, Y - cy) = atan2(dx, dy), measured from the y axis.
+template <typename T>
+__global__ void k_ref_shapes(T* __restrict__ phi, T* __restrict__ psi, const RefShape* __restrict__ sh, int V, int Nx,
+                             int Ny, int Nz, double dx, double dy, double dz, double eps) {
+  const long long NxNy = (long long)Nx * Ny, P = NxNy * Nz, tot = (long long)V * P;
+  const double den = 1.4142135623730951 * eps;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < tot; k += (long long)gridDim.x * blockDim.x) {
+    const int v = (int)(k / P);
+    const long long q = k - (long long)v * P;
+    const int l = (int)(q / NxNy);
+    const long long q2 = q - (long long)l * NxNy;
+    const int j = (int)(q2 / Nx), i = (int)(q2 - (long long)j * Nx);
+    const RefShape& s = sh[v];
+    const double X = i * dx - s.cx, Y = j * dy - s.cy;
+    double p = 0.0;
+    switch (s.kind) {
+      case RS_ELLIPSE: {                         // Init.jl:107-110
+        const double dist = sqrt(X * X / 2 + Y * Y);
+        p = tanh((s.R0 - dist) / den);
+        break;
+      }
+      case RS_TRIANGLE: {                        // Init.jl:112-127: smoothed max of three half-planes
+        const double ks = sqrt(3.0) / 2, kc = 0.5, sm = 40.0;
+        const double d1 = -Y, d2 = ks * X + kc * Y, d3 = -ks * X + kc * Y;
+        const double mx = fmax(d1, fmax(d2, d3));
+        const double ds = mx + (1 / sm) * log(exp(sm * (d1 - mx)) + exp(sm * (d2 - mx)) + exp(sm * (d3 - mx)));
+        p = -tanh((ds - s.R0 / 3) / den);
+        break;
+      }
+      case RS_STAR: {                            // Init.jl:128-139, 167-185
+        const double r = sqrt(X * X + Y * Y), th = atan2(X, Y);
+        p = tanh((s.R0 + s.amp * cos(10 * th) - r) / den);
+        break;
+      }
+      case RS_BLOB: {                            // Init.jl:140-160
+        const double r = sqrt(X * X + Y * Y), th = atan2(X, Y);
+        double R = s.R0;
+        for (int m = 0; m < 10; ++m) R += s.an[m] * s.R0 * cos((m + 1) * th + s.pn[m]);
+        p = tanh((R - r) / den);
+        break;
+      }
+      case RS_ELLIPSOID: {                       // Init_3d.jl:103-106
+        const double Z = l * dz - s.cz;
+        const double dist = sqrt(X * X / 2 + Y * Y / 2 + Z * Z);
+        p = tanh((s.R0 - dist) / den);
+        break;
+      }
+      default: break;
+    }
+    phi[k] = (T)p;
+    psi[k] = (T)(s.alpha * p + s.beta);
+  }
+}
+
 // Book-keeping of one step-graph capture: the kernels captured outside the
 // Krylov loops, and per loop (a WHILE node) the kernels of its body and the
 // device counter of its evaluated conditions (1 + iterations).
@@ -278,6 +348,7 @@ class Solver : public SolverBase {
   // device bookkeeping
   int *d_run_of = nullptr, *d_vbeg = nullptr;
   double *d_psi_in = nullptr, *d_psi_out = nullptr;
+  std::vector<int> h_run_sizes;
   Runs rn{};
   C* tab = nullptr;
   // state levels
@@ -343,6 +414,7 @@ class Solver : public SolverBase {
     for (int r = 0; r < R; ++r) { vbeg[r] = v; for (int k = 0; k < run_sizes[r]; ++k) run_of[v++] = r; }
     vbeg[R] = v;
     if (v != V) throw std::runtime_error("run sizes do not add up to the number of vesicle fields");
+    h_run_sizes.assign(run_sizes, run_sizes + R);
     d_run_of = dalloc<int>(V); d_vbeg = dalloc<int>(R + 1);
     d_psi_in = dalloc<double>(V); d_psi_out = dalloc<double>(V);
     VSAV_CUDA(cudaMemcpyAsync(d_run_of, run_of.data(), V * sizeof(int), cudaMemcpyHostToDevice, st));
@@ -1055,9 +1127,89 @@ class Solver : public SolverBase {
     for (int v = 0; v < V; ++v)
       if (shapes[v].nmodes < 0 || shapes[v].nmodes > 8 || !(shapes[v].a > 0) || !(shapes[v].b > 0))
         throw std::runtime_error("bad shape " + std::to_string(v) + ": need a, b > 0 and 0..8 modes");
+    if ((size_t)V * sizeof(Shape2D) > stage_bytes) throw std::runtime_error("too many vesicle fields for the staging buffer");
     VSAV_CUDA(cudaMemcpyAsync(stage, shapes, V * sizeof(Shape2D), cudaMemcpyHostToDevice, st));
     k_shapes2d<T><<<gridfor(VP), 256, 0, st>>>(phys4[0], phys4[0] + VP, reinterpret_cast<const Shape2D*>(stage), V, g.Nx,
                                                g.Ny, dm.Lx, dm.Ly, ph.eps); VSAV_COUNT_LAUNCH();
+    VSAV_LAUNCH_CHECK();
+    VSAV_CUDA(cudaMemsetAsync(uphys[0], 0, (g.nd + 1) * (long long)R * g.P * sizeof(T), st));
+    init_state(0);
+  }
+
+  // generate_initial_condition(conf, ops, state_type) (Init.jl:74-216, Init_3d.jl:67-152)
+  // for every run of the handle, each with its own N; blob_u: [R][20] uniform draws
+  // of state_type 4 (the reference's rand() calls, Init.jl:156-157), in draw order.
+  void init_reference_shapes(int state_type, int goal, const double* blob_u) override {
+    const int V = dm.V, R = dm.R;
+    const bool is3 = g.nd == 3, gs = goal == 's', gg = goal == 'g';
+    auto fail = [&](int r, const std::string& m) {
+      throw std::runtime_error("generate_initial_condition" + (R > 1 ? " (run " + std::to_string(r) + ")" : std::string()) +
+                               ": " + m);
+    };
+    std::vector<RefShape> sh(V);
+    std::memset(sh.data(), 0, V * sizeof(RefShape));
+    int v0 = 0;
+    for (int r = 0; r < R; ++r) {
+      const int N = h_run_sizes[r];
+      double cx[3], cy[3], cz[3];
+      if (N == 1) {
+        cx[0] = dm.Lx / 2; cy[0] = dm.Ly / 2; cz[0] = dm.Lz / 2;
+      } else if (N == 2) {
+        if (is3) { cx[0] = 0.73; cx[1] = 1.27; }                      // Init_3d.jl:89
+        else if (gg) { cx[0] = 0.75; cx[1] = 1.25; }                  // Init.jl:90-95
+        else if (gs) { cx[0] = 0.65; cx[1] = 1.35; }
+        else fail(r, "what's the goal? (N = 2 needs goal g or s)");
+        cy[0] = cy[1] = dm.Ly / 2; cz[0] = cz[1] = dm.Lz / 2;
+      } else if (N == 3) {
+        for (int n = 0; n < 3; ++n) { cx[n] = (n + 1) * dm.Lx / 4; cy[n] = dm.Ly / 2; cz[n] = dm.Lz / 2; }
+      } else {
+        fail(r, "N = " + std::to_string(N) + " has no vesicle centres (N <= 3)");
+      }
+      const std::string st = "state_type " + std::to_string(state_type);
+      if (N == 1 && state_type > 6) fail(r, st + " is invalid for N = 1");
+      if (N >= 2 && state_type <= 6 && !(is3 && N == 3)) fail(r, st + " is invalid for N = " + std::to_string(N));
+      for (int n = 0; n < N; ++n) {
+        RefShape& s = sh[v0 + n];
+        s.cx = cx[n]; s.cy = cy[n]; s.cz = cz[n];
+        s.alpha = gs ? -0.1 : -0.35;
+        s.beta = gs ? 0.7 : 0.45;
+        if (is3) {
+          if (N == 1 && state_type == 1) { s.kind = RS_ELLIPSOID; s.R0 = 0.2 * dm.Lx; }
+          if (N == 2 && state_type == 7) {
+            if (gs) fail(r, "state_type 7 needs goal g");
+            fail(r, "state_type 7 is not defined in 3D (the reference's branch uses the 2D grids X, Y)");
+          }
+          continue;
+        }
+        if (N == 1) {
+          if (state_type == 1) { s.kind = RS_ELLIPSE; s.R0 = 0.2 * dm.Lx; }
+          else if (state_type == 2) { s.kind = RS_TRIANGLE; s.R0 = 0.65 * dm.Lx; }
+          else if (state_type == 3) { s.kind = RS_STAR; s.R0 = gs ? 0.3 : 0.18; s.amp = gs ? 0.01 : 0.02; }
+          else if (state_type == 4) {
+            if (!blob_u) fail(r, "state_type 4 needs its 20 uniform draws per run");
+            s.kind = RS_BLOB; s.R0 = gs ? 0.3 : 0.2; s.amp = gs ? 0.15 : 0.25;
+            const double* u = blob_u + 20LL * r;
+            for (int m = 0; m < 10; ++m) {
+              s.an[m] = (u[2 * m] * 2 - 1) * s.amp / (m + 1);
+              s.pn[m] = u[2 * m + 1] * 2 * M_PI;
+            }
+          }
+        } else if (state_type == 7) {
+          if (gs) fail(r, "state_type 7 needs goal g");
+          s.kind = RS_STAR; s.R0 = 0.2; s.amp = 0.02;
+        } else if (state_type == 8) {
+          if (gg) fail(r, "state_type 8 needs goal s");
+          s.kind = RS_STAR; s.R0 = 0.3; s.amp = 0.01;
+        }
+      }
+      v0 += N;
+    }
+    if ((size_t)V * sizeof(RefShape) > stage_bytes) throw std::runtime_error("too many vesicle fields for the staging buffer");
+    const long long VP = (long long)V * g.P;
+    VSAV_CUDA(cudaMemcpyAsync(stage, sh.data(), V * sizeof(RefShape), cudaMemcpyHostToDevice, st));
+    k_ref_shapes<T><<<gridfor(VP), 256, 0, st>>>(phys4[0], phys4[0] + VP, reinterpret_cast<const RefShape*>(stage), V,
+                                                 g.Nx, g.Ny, g.Nz, dm.Lx / g.Nx, dm.Ly / g.Ny,
+                                                 is3 ? dm.Lz / g.Nz : 1.0, ph.eps); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     VSAV_CUDA(cudaMemsetAsync(uphys[0], 0, (g.nd + 1) * (long long)R * g.P * sizeof(T), st));
     init_state(0);

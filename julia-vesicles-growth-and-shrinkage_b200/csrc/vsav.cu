@@ -197,6 +197,12 @@ int vsav_init_shapes2d(vsav_handle* h, const vsav_shape2d* shapes) {
     return check_status(h, nullptr) < 0 ? VSAV_E_WC_NEGATIVE : VSAV_OK;
   });
 }
+int vsav_generate_initial_condition(vsav_handle* h, int32_t state_type, int32_t goal, const double* blob_u) {
+  return guard(h, [&] {
+    h->s->init_reference_shapes(state_type, goal, blob_u);
+    return check_status(h, nullptr) < 0 ? VSAV_E_WC_NEGATIVE : VSAV_OK;
+  });
+}
 int vsav_init_state(vsav_handle* h, int32_t hats_given) {
   return guard(h, [&] { h->s->init_state(hats_given); return check_status(h, nullptr) < 0 ? VSAV_E_WC_NEGATIVE : VSAV_OK; });
 }

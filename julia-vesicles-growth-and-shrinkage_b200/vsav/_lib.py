@@ -20,7 +20,7 @@ FIELD_ID = {k: i for i, k in enumerate(FIELDS)}
 # every function declared in include/vsav.h
 EXPORTS = ("vsav_create", "vsav_destroy", "vsav_last_error", "vsav_create_error", "vsav_default_options",
            "vsav_set_field", "vsav_get_field", "vsav_set_scalars", "vsav_get_scalars", "vsav_set_dt",
-           "vsav_get_dt", "vsav_set_A0", "vsav_get_A0", "vsav_init_state", "vsav_init_shapes2d", "vsav_step1", "vsav_step2", "vsav_step3",
+           "vsav_get_dt", "vsav_set_A0", "vsav_get_A0", "vsav_init_state", "vsav_init_shapes2d", "vsav_generate_initial_condition", "vsav_step1", "vsav_step2", "vsav_step3",
            "vsav_step4", "vsav_step5", "vsav_step6", "vsav_step7", "vsav_update_state", "vsav_run",
            "vsav_monitor", "vsav_get_work", "vsav_get_scalar_work", "vsav_transform", "vsav_time_run",
            "vsav_profile", "vsav_profile_read", "vsav_launch_count",
@@ -91,6 +91,7 @@ def load(path: str = LIB_PATH):
         "vsav_set_dt": ([H, D], ct.c_int),
         "vsav_get_dt": ([H, D], ct.c_int),
         "vsav_init_shapes2d": ([H, ct.POINTER(VsavShape2D)], ct.c_int),
+        "vsav_generate_initial_condition": ([H, ct.c_int32, ct.c_int32, D], ct.c_int),
         "vsav_set_A0": ([H, D], ct.c_int),
         "vsav_get_A0": ([H, D], ct.c_int),
         "vsav_init_state": ([H, i32], ct.c_int),

@@ -190,6 +190,21 @@ class Handle:
                 s.m[j], s.amp[j], s.phase[j] = int(m), float(amp), float(ph)
         self._chk(self.lib.vsav_init_shapes2d(self.h, arr))
 
+    def generate_initial_condition(self, state_type: int, goal: str = "s", blob_u=None):
+        """generate_initial_condition(conf, ops, state_type) (Init.jl:74-216,
+        Init_3d.jl:67-152) on the device for every run, then init_state's
+        initialisation.  goal: "g" or "s"; blob_u: for state_type 4, 20 uniform
+        draws per run ([R][20], the reference's rand() calls in order)."""
+        if goal not in ("g", "s"):
+            raise ValueError(f"what's the goal? now it is {goal}")
+        u = None
+        if blob_u is not None:
+            u = np.ascontiguousarray(blob_u, dtype=np.float64).reshape(-1)
+            if u.size != 20 * self.R:
+                raise ValueError(f"blob_u needs 20 draws per run ({20 * self.R}), got {u.size}")
+        self._chk(self.lib.vsav_generate_initial_condition(self.h, int(state_type), ord(goal),
+                                                           None if u is None else L.dptr(u)))
+
     def init_state(self, phi, psi, u=None, p=None):
         """generate_initial_condition's FFTs (Init.jl:199-216) + simulation.jl:22-53."""
         self.set_field("phi", phi)

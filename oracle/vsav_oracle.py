@@ -961,6 +961,122 @@ class Oracle:
 
 
 # ---------------------------------------------------------------------------
+# generate_initial_condition's shapes (Init.jl:74-197, Init_3d.jl:67-137)
+# ---------------------------------------------------------------------------
+class InitError(ValueError):
+    """The cases generate_initial_condition rejects (its error() calls, and the
+    UndefVarErrors of centres / 2D names it never defines)."""
+
+
+def reference_shapes(cfg: Config, state_type: int, blob_u=None):
+    """phi, psi [N][(Nz)][Ny][Nx] of generate_initial_condition(conf, ops,
+    state_type) (2D: Init.jl:74-197; 3D: Init_3d.jl:67-137).  blob_u: the 20
+    rand() values state_type 4 draws (Init.jl:155-159, in draw order: an, pn for
+    k = 1..10), which the reference takes from Julia's global RNG."""
+    N, eps, goal = cfg.N, cfg.epsilon, cfg.goal
+    Lx, Ly, dx, dy = cfg.Lx, cfg.Ly, cfg.dx, cfg.dy
+    den = SQ2 * eps
+    X = (np.arange(cfg.Nx) * dx)                      # range(0, Lx - dx, length=Nx), Init.jl:81-82
+    Y = (np.arange(cfg.Ny) * dy)
+    if cfg.ndim == 3:
+        Z = np.arange(cfg.Nz) * cfg.dz
+        X3, Y3, Z3 = X[None, None, :], Y[None, :, None], Z[:, None, None]
+        phi = np.zeros((N,) + cfg.shape)
+        if N == 1:                                    # Init_3d.jl:86-90
+            cx, cy, cz = [Lx / 2], [Ly / 2], [cfg.Lz / 2]
+        elif N == 2:
+            cx, cy, cz = [0.73, 1.27], [Ly / 2] * 2, [cfg.Lz / 2] * 2
+        elif N == 3:
+            cx, cy, cz = [Lx / 4, Lx / 2, 3 * Lx / 4], [Ly / 2] * 3, [cfg.Lz / 2] * 3
+        else:
+            raise InitError(f"N = {N}: no vesicle centres (Init_3d.jl:86-99 define N <= 3)")
+        if N == 1:                                    # Init_3d.jl:101-108
+            if state_type > 6:
+                raise InitError(f"state_type {state_type} is invalid for N = 1")
+            if state_type == 1:
+                R = 0.2 * Lx
+                dist = np.sqrt((X3 - cx[0]) ** 2 / 2 + (Y3 - cy[0]) ** 2 / 2 + (Z3 - cz[0]) ** 2)
+                phi[0] = np.tanh((R - dist) / den)
+        elif N == 2:                                  # Init_3d.jl:109-126
+            if state_type <= 6:
+                raise InitError(f"state_type {state_type} is invalid for N = 2")
+            if state_type == 7:
+                if goal == "s":
+                    raise InitError("state_type 7 needs goal g")
+                raise InitError("state_type 7 is not defined in 3D (Init_3d.jl:118-125 use the 2D names X, Y)")
+    else:
+        X2, Y2 = X[None, :], Y[:, None]
+        phi = np.zeros((N,) + cfg.shape)
+        if N == 1:                                    # Init.jl:86-100
+            cx, cy = [Lx / 2], [Ly / 2]
+        elif N == 2:
+            if goal == "g":
+                cx = [0.75, 1.25]
+            elif goal == "s":
+                cx = [0.65, 1.35]
+            else:
+                raise InitError(f"what's the goal? now it is {goal}")
+            cy = [Ly / 2, Ly / 2]
+        elif N == 3:
+            cx, cy = [Lx / 4, Lx / 2, 3 * Lx / 4], [Ly / 2] * 3
+        else:
+            raise InitError(f"N = {N}: no vesicle centres (Init.jl:86-100 define N <= 3)")
+
+        def star(n, R0, amp, k=10):
+            ddx, ddy = X2 - cx[n], Y2 - cy[n]
+            r = np.sqrt(ddx ** 2 + ddy ** 2)
+            theta = np.arctan2(ddx, ddy)              # Julia atan(X - cx, Y - cy)
+            return np.tanh((R0 + amp * np.cos(k * theta) - r) / den)
+
+        if N == 1:                                    # Init.jl:102-160
+            if state_type > 6:
+                raise InitError(f"state_type {state_type} is invalid for N = 1")
+            ddx, ddy = X2 - cx[0], Y2 - cy[0]
+            if state_type == 1:                       # ellipse
+                R = 0.2 * Lx
+                dist = np.sqrt(ddx ** 2 / 2 + ddy ** 2)
+                phi[0] = np.tanh((R - dist) / den)
+            elif state_type == 2:                     # smoothed triangle
+                radius, sm = 0.65 * Lx, 40.0
+                ks, kc = math.sqrt(3) / 2, 0.5
+                d1 = -ddy + 0 * ddx
+                d2 = ks * ddx + kc * ddy
+                d3 = -ks * ddx + kc * ddy
+                mx = np.maximum(d1, np.maximum(d2, d3))
+                ds = mx + (1 / sm) * np.log(np.exp(sm * (d1 - mx)) + np.exp(sm * (d2 - mx)) + np.exp(sm * (d3 - mx)))
+                phi[0] = -np.tanh((ds - radius / 3) / den)
+            elif state_type == 3:                     # star
+                R0, amp = (0.3, 0.01) if goal == "s" else (0.18, 0.02)
+                phi[0] = star(0, R0, amp)
+            elif state_type == 4:                     # random blob
+                R0, amp = (0.3, 0.15) if goal == "s" else (0.2, 0.25)
+                if blob_u is None or len(blob_u) < 20:
+                    raise InitError("state_type 4 needs its 20 uniform draws")
+                r = np.sqrt(ddx ** 2 + ddy ** 2)
+                theta = np.arctan2(ddx, ddy)
+                R = np.full(theta.shape, R0)
+                for k in range(1, 11):
+                    an = (blob_u[2 * k - 2] * 2 - 1) * amp / k
+                    pn = blob_u[2 * k - 1] * 2 * math.pi
+                    R = R + an * R0 * np.cos(k * theta + pn)
+                phi[0] = np.tanh((R - r) / den)
+        else:                                         # Init.jl:161-189
+            if state_type <= 6:
+                raise InitError(f"state_type {state_type} is invalid for N = {N}")
+            for n in range(N):
+                if state_type == 7:
+                    if goal == "s":
+                        raise InitError("state_type 7 needs goal g")
+                    phi[n] = star(n, 0.2, 0.02)
+                elif state_type == 8:
+                    if goal == "g":
+                        raise InitError("state_type 8 needs goal s")
+                    phi[n] = star(n, 0.3, 0.01)
+    psi = -0.1 * phi + 0.7 if goal == "s" else -0.35 * phi + 0.45   # Init.jl:191-197
+    return phi, psi
+
+
+# ---------------------------------------------------------------------------
 # initialisation: simulation.jl:22-53 (with a given initial phi/psi)
 # ---------------------------------------------------------------------------
 def make_state(cfg: Config, phi: np.ndarray, psi: np.ndarray, ops: Operators) -> FieldState:
