@@ -455,28 +455,37 @@ def run_ensemble(args):
 
 def run_config(args):
     """Other configurations of the path, each its own JSON line (not the headline):
-    multi2d_512x4 (2D 512^2, 4 vesicles) and single3d_128 (3D 128^3, spectral-direct
-    psi): FP64 GPU, the faster GPU precision with its per-field error against the
-    FP64 GPU path, and the CPU restatement (oracle) on a bounded sample."""
+    multi2d_512x4 (2D 512^2, 4 vesicles), single3d_128 (3D 128^3, spectral-direct
+    psi) and single3d_128_psivar (the same with the variable psi mobility and its
+    BiCGSTAB, an extension): FP64 GPU, the faster GPU precision with its per-field
+    error against the FP64 GPU path, and the CPU restatement (oracle) on a
+    bounded sample."""
     from vsav import Handle, ics
     from oracle import vsav_oracle as O
-    kw, phi, psi, _ = ics.workload(args.workload, seed=0)
+    variable = args.workload.endswith("_psivar")
+    kw, phi, psi, _ = ics.workload(args.workload.replace("_psivar", ""), seed=0)
     # 2D: the headline's dt; 3D: 1e-5 (both inside the range where the oracle's modified energy decreases)
     kw["dt"] = DT if kw.get("Nz", 0) == 0 else 1e-5
     fast = "mixed" if args.workload == "multi2d_512x4" else "fp32"
     out = {"workload": args.workload, "metric": "steps/s", "unit": "steps/s", "steps": args.steps,
            "warmup": args.warmup, "dt": kw["dt"], "grid": [kw["Nx"], kw["Ny"]] + ([kw["Nz"]] if kw.get("Nz") else []),
-           "vesicles": kw["N"]}
+           "vesicles": kw["N"], "psi3d_variable": variable}
     ref = None
     for prec in ("fp64", fast):
-        h = Handle(Cfg(**kw), precision=prec)
+        xo = dict(psi3d_variable=True) if variable else {}
+        if variable and prec == "fp32":
+            # the tightest tolerance one FP32 solve reaches reliably (the mixed 2D mode's sweep floor)
+            xo.update(psi_rtol=1e-6, psi_itmax=60)
+        h = Handle(Cfg(**kw), precision=prec, **xo)
         h.init_state(phi, psi)
         E, _ = h.run(1, args.warmup, monitor=True)
         fields = {k: h.get_field(k) for k in ("phi", "psi", "mu", "nu", "u", "p")}
         ms = h.time_run(1 + args.warmup, args.steps, monitor=True)
-        h.close()
         res = {"value": args.steps / (ms / 1000.0), "ms_per_step": ms / args.steps,
                "energy_non_increasing": bool(np.all(np.diff(E[:, 0]) <= 0))}
+        if variable:
+            res["psi_iters_last_step"] = [int(x) for x in h.psi_stats()[:, 0]]
+        h.close()
         if ref is None:
             ref = fields
         else:
@@ -486,7 +495,7 @@ def run_config(args):
     if not args.no_cpu:
         cfg = O.Config(**kw)
         cores = os.cpu_count() or 1
-        orc = O.Oracle(cfg, workers=cores)
+        orc = O.Oracle(cfg, workers=cores, psi3d_variable=variable)
         pres = O.make_state(cfg, phi, psi, orc.ops)
         O.init_state(cfg, pres, orc.ops)
         old = pres.copy()
@@ -513,13 +522,14 @@ def main():
                     help="the configuration of the headline value")
     ap.add_argument("--arms", default="", help="comma-separated subset of the compared configurations")
     ap.add_argument("--workload", default="multi2d_1024x8",
-                    choices=["multi2d_1024x8", "ensemble_256x64", "multi2d_512x4", "single3d_128"],
+                    choices=["multi2d_1024x8", "ensemble_256x64", "multi2d_512x4", "single3d_128",
+                             "single3d_128_psivar"],
                     help="anything but multi2d_1024x8 prints its own comparison line, not the headline")
     args = ap.parse_args()
     if args.workload == "ensemble_256x64":
         run_ensemble(args)
         return
-    if args.workload in ("multi2d_512x4", "single3d_128"):
+    if args.workload in ("multi2d_512x4", "single3d_128", "single3d_128_psivar"):
         run_config(args)
         return
     if args.impl == "reference":

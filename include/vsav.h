@@ -71,6 +71,10 @@ typedef struct vsav_options {
   int32_t device;               /* CUDA device ordinal */
   int32_t graph;                /* 1 (default): vsav_run replays each time step after the first as one
                                    CUDA graph (Krylov loops as conditional nodes); 0: eager launches */
+  int32_t psi3d_variable;       /* 3D only.  0 (default): psi by the reference's constant-M0_psi spectral
+                                   division (Solvers_3d.jl:28-30); 1: the 2D scheme's variable mobility
+                                   M_psi(phi*) (Utils_3d.jl:20) and its diagonal-preconditioned BiCGSTAB
+                                   (Solvers.jl:26-81) on 3D full spectra -- no counterpart in the reference */
 } vsav_options;
 
 /* field ids (FieldState, src/Types.jl:167-201) */

@@ -444,6 +444,7 @@ __global__ void __launch_bounds__(NT, MinB<E, NT>::v) k_rows_c2c(const cplx<T>* 
 // geo selects how (kx,ky,kz) are decoded for the multiplier:
 //   0: 2D y pass (kx=c, ky=e)   1: 3D z pass (kx=c%kp, ky=c/kp, kz=e)
 //   2: 3D y pass (kx=c, ky=e, kz=o%Nz)   3: 2D full-spectrum y pass (kx=c in [0,Nx))
+//   4: 3D full-spectrum z pass (kx=c%Nx, ky=c/Nx, kz=e)   5: 3D full-spectrum y pass (kx=c, ky=e, kz=o%Nz)
 // ---------------------------------------------------------------------------
 struct ColArgs {
   int logL, S, W, TW, logTW, tiles;
@@ -461,6 +462,12 @@ __device__ __forceinline__ C col_mult(const ColArgs& a, int mult, double ms, int
     case 0: kx = c; ky = kfreq(e, a.Ny); break;
     case 1: kx = c % a.kp; ky = kfreq(c / a.kp, a.Ny); kz = kfreq(e, a.Nz); break;
     case 2: kx = c; ky = kfreq(e, a.Ny); kz = kfreq((int)(o % a.Nz), a.Nz); break;
+    case 4: {
+      const int cx = c & (a.Nx - 1);
+      kx = (mult == M_DX0) ? kfreq(cx, a.Nx) : (double)cx; ky = kfreq(c / a.Nx, a.Ny); kz = kfreq(e, a.Nz);
+      break;
+    }
+    case 5: kx = (mult == M_DX0) ? kfreq(c, a.Nx) : (double)c; ky = kfreq(e, a.Ny); kz = kfreq((int)(o % a.Nz), a.Nz); break;
     default: kx = (mult == M_DX0) ? kfreq(c, a.Nx) : (double)c; ky = kfreq(e, a.Ny); break;
   }
   if (mult == M_DXZ && (int)kx == a.Nx / 2) return mk<C>(0.0, 0.0);

@@ -315,7 +315,8 @@ template <typename T>
 __global__ void k_step1_k(const cplx<T>* __restrict__ hp, const cplx<T>* __restrict__ ho, const cplx<T>* __restrict__ Hh,
                           const cplx<T>* __restrict__ fl, int nfl, const cplx<T>* __restrict__ adv,
                           cplx<T>* __restrict__ cache, cplx<T>* __restrict__ rhs,
-                          const double* __restrict__ dtv, double a, double b, double c, Phys ph, Runs rn, Geom g) {
+                          const double* __restrict__ dtv, double a, double b, double c, Phys ph, Runs rn, Geom g,
+                          int psi_div) {
   using C = cplx<T>;
   const long long VH = (long long)rn.V * g.H;
   K_LOOP(VH, i) {
@@ -357,7 +358,7 @@ __global__ void k_step1_k(const cplx<T>* __restrict__ hp, const cplx<T>* __restr
       f12 = f12 + make_double2(-kv * fd.y, kv * fd.x);
     }
     double2 r21 = make_double2(-B.x, -B.y);
-    if (g.nd == 2) {
+    if (!psi_div) {                       // right-hand sides of the psi BiCGSTAB
       C o;
       o.x = rp.x; o.y = rp.y; rhs[i] = o;
       o.x = f12.x; o.y = f12.y; rhs[VH + i] = o;

@@ -127,11 +127,17 @@ struct VGeom {
   int Nx, Ny, kp, nkx, logNx;
   long long n;      // slots per field
   double kxs, kys;
+  int nd3 = 0;      // 1: 3D full spectra [Nz][Ny][Nx] (the 3D variable-mobility solve)
+  int logNy = 0, Nz = 1;
+  double kzs = 0.0;
 };
 __device__ __forceinline__ void vk(const VGeom& g, long long s, int& kx, int& ky, double& kxv, double& kyv, double& w) {
   // slot < 2^31 within a field: 32-bit index arithmetic (row lengths are powers of two or kp)
   const unsigned su = (unsigned)s;
-  if (g.full) { kx = (int)(su & (unsigned)(g.Nx - 1)); ky = (int)(su >> g.logNx); }
+  if (g.full) {
+    kx = (int)(su & (unsigned)(g.Nx - 1)); ky = (int)(su >> g.logNx);
+    if (g.nd3) ky &= g.Ny - 1;
+  }
   else { ky = (int)(su / (unsigned)g.kp); kx = (int)(su - (unsigned)ky * (unsigned)g.kp); }
   kyv = kfreq(ky, g.Ny) * g.kys;
   if (g.full) { kxv = kfreq(kx, g.Nx) * g.kxs; w = 1.0; }
@@ -139,6 +145,13 @@ __device__ __forceinline__ void vk(const VGeom& g, long long s, int& kx, int& ky
     kxv = kx * g.kxs;
     w = (kx >= g.nkx) ? 0.0 : ((kx == 0 || kx == g.Nx / 2) ? 1.0 : 2.0);
   }
+}
+
+// kz^2 of a 3D full-spectrum slot (0 in 2D)
+__device__ __forceinline__ double vk_kz2(const VGeom& g, long long s) {
+  if (!g.nd3) return 0.0;
+  const double kzv = kfreq((int)((unsigned)s >> (g.logNx + g.logNy)), g.Nz) * g.kzs;
+  return kzv * kzv;
 }
 
 // y = a_dt * x - ( m_x t1 + i ky t2 ) at slot s of field f (HALF: Nyquist x multiplier zero)
@@ -386,6 +399,56 @@ __global__ void __launch_bounds__(NT, MinB<E, NT>::v) k_psi_cols_comb(const cplx
   block_reduce_store<4>(acc, part + ((long long)f * a.tiles + tile) * 4, smm);
 }
 
+// The 3D full-spectrum operator output (the 2D FULL form with a z direction):
+//   y = P^-1 ( a_dt x - (i kx0 t1 + i ky t2 + i kz t3) ),  P^-1 = 1/(a_dt + Mmax S4 k^2) or 1,
+// with k_psi_combine's modes and dot products.  t1..t3 hold F fields each.
+template <typename T>
+__global__ void __launch_bounds__(256) k_psi_combine3(const cplx<T>* __restrict__ x, const cplx<T>* __restrict__ t1,
+                                                      const cplx<T>* __restrict__ t2, const cplx<T>* __restrict__ t3,
+                                                      cplx<T>* __restrict__ y, const cplx<T>* __restrict__ cvec,
+                                                      const cplx<T>* __restrict__ svec, int mode,
+                                                      const double* __restrict__ adt_r, const double* __restrict__ mmax_r,
+                                                      double S4, VGeom g, SysMap sm, const int* __restrict__ active, EW ew,
+                                                      double2* part) {
+  __shared__ double smm[2 * 4 * 8];
+  KSum acc[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+  const int f = blockIdx.y;
+  if (!active || active[sm.sys(f)]) {
+    const int r = sm.run_of[f % sm.V];
+    const double adt = adt_r[r], mm = mmax_r ? mmax_r[r] : 0.0;
+    const long long beg = (long long)blockIdx.x * ew.chunk, end = min(ew.n, beg + ew.chunk);
+    for (long long s = beg + threadIdx.x; s < end; s += blockDim.x) {
+      const unsigned su = (unsigned)s;
+      const double kxv = kfreq((int)(su & (unsigned)(g.Nx - 1)), g.Nx) * g.kxs;
+      const double kyv = kfreq((int)((su >> g.logNx) & (unsigned)(g.Ny - 1)), g.Ny) * g.kys;
+      const double kzv = kfreq((int)(su >> (g.logNx + g.logNy)), g.Nz) * g.kzs;
+      const long long j = (long long)f * g.n + s;
+      const cplx<T> xv = x ? x[j] : cplx<T>{}, a = t1[j], b = t2[j], c = t3[j];
+      const double dx = -(kxv * (double)a.y + kyv * (double)b.y + kzv * (double)c.y);
+      const double dy = kxv * (double)a.x + kyv * (double)b.x + kzv * (double)c.x;
+      double ox = adt * (double)xv.x - dx, oy = adt * (double)xv.y - dy;
+      if (mmax_r) {
+        const double pinv = 1.0 / (adt + mm * S4 * (kxv * kxv + kyv * kyv + kzv * kzv));
+        ox *= pinv; oy *= pinv;
+      }
+      cplx<T> ot; ot.x = ox; ot.y = oy;
+      y[j] = ot;
+      ox = ot.x; oy = ot.y;                                 // the dots use the stored (rounded) values
+      if (mode == 0) {
+        const cplx<T> cv = cvec[j];
+        acc[0].add((double)cv.x * ox + (double)cv.y * oy);
+        acc[1].add((double)cv.x * oy - (double)cv.y * ox);
+      } else {
+        const cplx<T> sv = svec[j];
+        acc[0].add(ox * (double)sv.x + oy * (double)sv.y);
+        acc[1].add(ox * (double)sv.y - oy * (double)sv.x);
+        acc[2].add(ox * ox + oy * oy);
+      }
+    }
+  }
+  block_reduce_store<4>(acc, part + ((long long)f * ew.bpf + blockIdx.x) * 4, smm);
+}
+
 // r = M^-1 b, x = 0, p = r, dots <b, r>, ||r||^2  (Krylov.jl bicgstab initialisation)
 template <typename T>
 __global__ void __launch_bounds__(256) k_psi_init(const cplx<T>* __restrict__ b, cplx<T>* __restrict__ x, cplx<T>* __restrict__ r,
@@ -407,7 +470,7 @@ __global__ void __launch_bounds__(256) k_psi_init(const cplx<T>* __restrict__ b,
     if (w == 0.0) { r[j] = z; p[j] = z; continue; }
     cplx<T> bv = b[j];
     double kxp = (!g.full && kx == g.Nx / 2) ? 0.0 : kxv;
-    double pinv = mmax_r ? 1.0 / (adt + mm * S4 * (kxp * kxp + kyv * kyv)) : 1.0;
+    double pinv = mmax_r ? 1.0 / (adt + mm * S4 * (kxp * kxp + kyv * kyv + vk_kz2(g, s))) : 1.0;
     cplx<T> rv; rv.x = (double)bv.x * pinv; rv.y = (double)bv.y * pinv;
     r[j] = rv; p[j] = rv;
     acc[0].add(w * ((double)bv.x * (double)rv.x + (double)bv.y * (double)rv.y));

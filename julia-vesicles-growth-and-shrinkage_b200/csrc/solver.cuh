@@ -34,6 +34,7 @@ struct Options {
   int psi_refine_min = 1;    // least refinement sweeps of the mixed mode
   double psi_inner_rtol = 1e-6;   // tightest relative tolerance of one FP32 sweep
   int graph = 1;             // vsav_run replays each time step as a CUDA graph
+  int psi3d_var = 0;         // 3D: variable psi mobility + BiCGSTAB (the 2D scheme) instead of the constant-M0 division
 };
 
 struct StepStatus {
@@ -362,14 +363,14 @@ class Solver : public SolverBase {
   double2* part;
   int* d_err;
   // psi solver
-  C *vb, *vx, *vr, *vp, *vv, *vs, *vt, *vt12;
+  C *vb = nullptr, *vx = nullptr, *vr = nullptr, *vp = nullptr, *vv = nullptr, *vs = nullptr, *vt = nullptr, *vt12 = nullptr;
   C *vph = nullptr, *vsh = nullptr;          // preconditioned directions (flexible BiCGSTAB)
   uint32_t* nfrag = nullptr;                 // learned preconditioner weights (mma fragments)
   float *nbias = nullptr, *inv_s = nullptr;
   bool net_ok = false;
   float* hv = nullptr;                       // harvested iterates
   int hv_cap = 0, hv_count = 0;
-  BiState* bst; int *bupd, *d_any;
+  BiState* bst = nullptr; int *bupd = nullptr, *d_any = nullptr;
   int* h_pinned_any = nullptr;
   StepStatus last;
   double* stage = nullptr;   // host-format staging
@@ -464,10 +465,13 @@ class Solver : public SolverBase {
     long long bpf = (nmaxe + 2047) / 2048;
     part = dalloc<double2>(bpf * std::max(3 * V, R) * 32);
     d_err = dalloc<int>(1);
-    if (nd == 2) {
+    if (nd == 2 || opt.psi3d_var) {
       long long n = psi_n();
+      if (nd == 3 && (!psi_full() || opt.psi_precond != 0 || opt.psi_mixed))
+        throw std::runtime_error("the 3D variable-mobility psi solve is the full-spectrum, diagonal-preconditioned form");
       vb = dalloc<C>(3 * V * n); vr = dalloc<C>(3 * V * n); vp = dalloc<C>(3 * V * n);
-      vv = dalloc<C>(3 * V * n); vs = dalloc<C>(3 * V * n); vt = dalloc<C>(3 * V * n); vt12 = dalloc<C>(6 * V * n);
+      vv = dalloc<C>(3 * V * n); vs = dalloc<C>(3 * V * n); vt = dalloc<C>(3 * V * n);
+      vt12 = dalloc<C>((nd == 3 ? 9 : 6) * V * n);
       vx = psi_full() ? dalloc<C>(3 * V * n) : nullptr;
       bst = dalloc<BiState>(3 * R); bupd = dalloc<int>(3 * R); d_any = dalloc<int>(1);
       VSAV_CUDA(cudaMallocHost(&h_pinned_any, sizeof(int)));
@@ -626,7 +630,7 @@ class Solver : public SolverBase {
       prof.end(st, KC_ROWS_C2C, (double)nrows * g.Nx * ((in_real ? sizeof(T) : sizeof(C)) + sizeof(C)));
     })
   }
-  // geo: 0 2D y (half), 1 3D z (half), 2 3D y (half), 3 2D y (full)
+  // geo: 0 2D y (half), 1 3D z (half), 2 3D y (half), 3 2D y (full), 4 3D z (full), 5 3D y (full)
   ColArgs colargs(int geo, long long& nouter, int E, int NT) const {
     ColArgs a{};
     a.geo = geo; a.Nx = g.Nx; a.Ny = g.Ny; a.Nz = g.Nz; a.kp = g.kp;
@@ -635,6 +639,8 @@ class Solver : public SolverBase {
     if (geo == 0) { L = g.Ny; a.S = g.kp; a.W = g.kp; a.O = (long long)g.Ny * g.kp; a.kpv = g.kp; a.nkv = g.nkx; }
     else if (geo == 1) { L = g.Nz; a.S = g.Ny * g.kp; a.W = g.Ny * g.kp; a.O = g.H; a.kpv = g.kp; a.nkv = g.nkx; }
     else if (geo == 2) { L = g.Ny; a.S = g.kp; a.W = g.kp; a.O = (long long)g.Ny * g.kp; a.kpv = g.kp; a.nkv = g.nkx; nouter *= g.Nz; }
+    else if (geo == 4) { L = g.Nz; a.S = g.Ny * g.Nx; a.W = g.Ny * g.Nx; a.O = g.Pfull; a.kpv = g.Nx; a.nkv = g.Nx; }
+    else if (geo == 5) { L = g.Ny; a.S = g.Nx; a.W = g.Nx; a.O = (long long)g.Ny * g.Nx; a.kpv = g.Nx; a.nkv = g.Nx; nouter *= g.Nz; }
     else { L = g.Ny; a.S = g.Nx; a.W = g.Nx; a.O = (long long)g.Ny * g.Nx; a.kpv = g.Nx; a.nkv = g.Nx; }
     a.logL = ilog2(L);
     int TW = std::max(1, E * NT / L);
@@ -653,7 +659,8 @@ class Solver : public SolverBase {
       int thr = std::max(a.TW, a.TW * L / E_);
       size_t sm = 2 * (size_t)col_tile_elems(L, a.TW, ilog2(E_)) * sizeof(C);
       long long grid = (long long)a.tiles * nouter;
-      long long valid_lines = (geo == 3) ? (long long)g.Nx : (long long)g.nkx * (geo == 1 ? g.Ny : 1);
+      long long valid_lines = (geo == 3 || geo == 5) ? (long long)g.Nx
+                              : (geo == 4 ? (long long)g.Ny * g.Nx : (long long)g.nkx * (geo == 1 ? g.Ny : 1));
       double cb = (double)nouter * valid_lines * L * sizeof(C) * ((in1 ? 2 : 1) + 1);
       prof.begin(st);
       if (inv) {
@@ -669,7 +676,8 @@ class Solver : public SolverBase {
     })
   }
   void rows_mul(C* t, long long nrows, bool full, int f0 = 0, int fc = 0) {
-    if (fc == 0) fc = (int)(nrows / (2 * g.Ny));
+    const int rpf = g.Nz * g.Ny;                          // rows of one field
+    if (fc == 0) fc = (int)(nrows / (2 * rpf));
     int L = full ? g.Nx : g.Nx / 2, logL = ilog2(L);
     SysMap sm{dm.V, dm.R, d_run_of};
     int rowlen = full ? g.Nx : g.kp;
@@ -683,11 +691,11 @@ class Solver : public SolverBase {
       if (full) {
         set_smem_attr<E_, NT_>((const void*)k_rows_mul<T, E_, NT_, true>, smb);
         k_rows_mul<T, E_, NT_, true><<<(unsigned)grid, thr, smb, st>>>(t, Mpsi, (T)0, (T)(1.0 / g.P), logL, lognl, nrows,
-                                                                       rowlen, g.Ny, sm, bupd, f0, fc, tab);
+                                                                       rowlen, rpf, sm, bupd, f0, fc, tab);
       } else {
         set_smem_attr<E_, NT_>((const void*)k_rows_mul<T, E_, NT_, false>, smb);
         k_rows_mul<T, E_, NT_, false><<<(unsigned)grid, thr, smb, st>>>(t, Mpsi, (T)0, (T)(1.0 / g.P), logL, lognl, nrows,
-                                                                        rowlen, g.Ny, sm, bupd, f0, fc, tab);
+                                                                        rowlen, rpf, sm, bupd, f0, fc, tab);
       }
       VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
@@ -899,9 +907,9 @@ class Solver : public SolverBase {
     // psi 12 flux: D1_d . rfft(M dG/dx_d)
     const C* Gh = Hh + 3 * VH;
     for (int d = 0; d < nd; ++d) irfft(Gh, V, gG + d * VP, M_DX + d);
-    if (nd == 2) {
-      k_mul_field<T><<<gridfor(VP), 256, 0, st>>>(gG, Mpsi, 1.0, gG, VP, 1); VSAV_COUNT_LAUNCH();
-      k_mul_field<T><<<gridfor(VP), 256, 0, st>>>(gG + VP, Mpsi, 1.0, gG + VP, VP, 1); VSAV_COUNT_LAUNCH();
+    const bool psi_krylov_step = nd == 2 || opt.psi3d_var;
+    if (psi_krylov_step) {
+      k_mul_field<T><<<gridfor((long long)nd * VP), 256, 0, st>>>(gG, Mpsi, 1.0, gG, VP, nd); VSAV_COUNT_LAUNCH();
     } else {
       k_mul_field<T><<<gridfor(3 * VP), 256, 0, st>>>(gG, nullptr, ph.M0_psi, gG, 3 * VP, 1); VSAV_COUNT_LAUNCH();
     }
@@ -916,9 +924,9 @@ class Solver : public SolverBase {
     rfft(adv, 2LL * V, advh);
     k_set_adt<<<(R + 63) / 64, 64, 0, st>>>(d_dt, cur_a, d_adt, R); VSAV_COUNT_LAUNCH();
     k_step1_k<T><<<gridfor(VH), 256, 0, st>>>(hat4[0], hat4[1], Hh, flh, nd, advh, cache, rhs, d_dt, cur_a, cur_b, cur_c,
-                                              ph, rn, g); VSAV_COUNT_LAUNCH();
+                                              ph, rn, g, psi_krylov_step ? 0 : 1); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
-    if (nd == 2) {
+    if (psi_krylov_step) {
       psi_solve();
       k_nu<T><<<gridfor(VH), 256, 0, st>>>(cache, Gh, ph.S4, VH, g); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
@@ -1261,6 +1269,7 @@ class Solver : public SolverBase {
   EW dot_ew{};                 // partial layout of the dots of the last matvec
   bool fused_ops = true;       // FULL form: fused column passes (VSAV_PSI_FUSED=0: separate kernels)
   void matvec(const C* in, C* out, int mode, const C* svec, bool precond = true) {
+    if (g.nd == 3) { matvec3(in, out, mode, svec, precond); return; }
     const int V = dm.V;
     const long long F = 3LL * V, n = psi_n();
     const bool full = psi_full();
@@ -1295,10 +1304,42 @@ class Solver : public SolverBase {
     }
   }
 
+  // 3D full-spectrum operator (variable mobility): per direction d the inverse
+  // z and y passes of i k_d S4 x, then one x pass (inverse, * M_psi / P,
+  // forward) and the forward y and z passes over all three, then the combine.
+  void matvec3(const C* in, C* out, int mode, const C* svec, bool precond) {
+    const int V = dm.V;
+    const long long F = 3LL * V, n = psi_n();
+    EW e = ew(n);
+    SysMap sm{V, dm.R, d_run_of};
+    const double* pre = precond ? mmax_r : nullptr;
+    dot_ew = e;
+    C* t = vt12;                                          // [3][F][n]
+    const int mults[3] = {M_DX0, M_DY, M_DZ};
+    for (int d = 0; d < 3; ++d) {
+      cols(true, 4, F, in, nullptr, 1, 0, mults[d], ph.S4, t + d * F * n, 1);
+      cols(true, 5, F, t + d * F * n, nullptr, 1, 0, M_ONE, 1, t + d * F * n, 1);
+    }
+    rows_mul(t, 3 * F * g.Nz * g.Ny, true, 0, (int)F);
+    cols(false, 5, 3 * F, t, nullptr, 1, 0, M_ONE, 1, t, 1);
+    cols(false, 4, 3 * F, t, nullptr, 1, 0, M_ONE, 1, t, 1);
+    prof.begin(st);
+    k_psi_combine3<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(in, t, t + F * n, t + 2 * F * n, out, vb, svec, mode, d_adt,
+                                                                pre, ph.S4, vgeom(), sm, bupd, e, part); VSAV_COUNT_LAUNCH();
+    VSAV_LAUNCH_CHECK();
+    prof.end(st, KC_PSI_VEC, (double)F * n * 6.0 * sizeof(C));
+  }
+
   // b = fft(irfft(rhs)) (FULL) / rfft(irfft(rhs)) (HALF)   (Solvers.jl:70-71)
   void psi_prepare_b() {
     const long long F = 3LL * dm.V;
     irfft(rhs, F, tmpP);
+    if (g.nd == 3) {
+      rows_c2c<false>(nullptr, tmpP, vb, 1.0, F * g.Nz * g.Ny);
+      cols(false, 5, F, vb, nullptr, 1, 0, M_ONE, 1, vb, 1);
+      cols(false, 4, F, vb, nullptr, 1, 0, M_ONE, 1, vb, 1);
+      return;
+    }
     if (psi_full()) {
       rows_c2c<false>(nullptr, tmpP, vb, 1.0, F * g.Ny);
       cols(false, 3, F, vb, nullptr, 1, 0, M_ONE, 1, vb, 1);
@@ -1309,7 +1350,11 @@ class Solver : public SolverBase {
   C* psi_x() { return psi_full() ? vx : cache + 5LL * dm.V * g.H; }
   void psi_finish() {
     const long long F = 3LL * dm.V, VH = (long long)dm.V * g.H;
-    if (psi_full()) { k_trunc<T><<<gridfor(F * g.Ny * g.kp), 256, 0, st>>>(vx, cache + 5 * VH, g.Nx, g.Ny, g.kp, g.nkx, (int)F); VSAV_COUNT_LAUNCH(); VSAV_LAUNCH_CHECK(); }
+    if (psi_full()) {
+      const int rows = g.Nz * g.Ny;
+      k_trunc<T><<<gridfor(F * rows * g.kp), 256, 0, st>>>(vx, cache + 5 * VH, g.Nx, rows, g.kp, g.nkx, (int)F); VSAV_COUNT_LAUNCH();
+      VSAV_LAUNCH_CHECK();
+    }
   }
   void psi_solve() {
     if (opt.psi_mixed) { psi_solve_mixed(); return; }
@@ -1398,7 +1443,7 @@ class Solver : public SolverBase {
     const long long F = 3LL * V, n = psi_n();
     const bool full = psi_full();
     EW e = ew(n);
-    VGeom vg{full ? 1 : 0, g.Nx, g.Ny, g.kp, g.nkx, ilog2(g.Nx), n, g.kxs, g.kys};
+    VGeom vg = vgeom();
     SysMap sm{V, R, d_run_of};
     k_psi_init<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(vb, x, vr, vp, d_adt, mmax_r, ph.S4, vg, sm, e, part); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
@@ -1438,7 +1483,9 @@ class Solver : public SolverBase {
   //   x += alpha p^ + omega s^; r = s - omega t; beta = (rho'/rho)(alpha/omega)
   //   p = r + beta (p - omega v)
   VGeom vgeom() const {
-    return VGeom{psi_full() ? 1 : 0, g.Nx, g.Ny, g.kp, g.nkx, ilog2(g.Nx), psi_n(), g.kxs, g.kys};
+    VGeom v{psi_full() ? 1 : 0, g.Nx, g.Ny, g.kp, g.nkx, ilog2(g.Nx), psi_n(), g.kxs, g.kys};
+    if (g.nd == 3) { v.nd3 = 1; v.logNy = ilog2(g.Ny); v.Nz = g.Nz; v.kzs = g.kzs; }
+    return v;
   }
   void psi_flex(C* x, double rtol, int itmax) {
     const int V = dm.V, R = dm.R, S = 3 * R;
@@ -1644,6 +1691,7 @@ class Solver : public SolverBase {
   void get_scalar_work(int what, double* out) override {
     const int R = dm.R, V = dm.V;
     if (what == 5) {
+      if (!bst) throw std::runtime_error("this handle has no psi BiCGSTAB (3D with constant mobility)");
       std::vector<BiState> hb(3 * R);
       VSAV_CUDA(cudaMemcpyAsync(hb.data(), bst, 3 * R * sizeof(BiState), cudaMemcpyDeviceToHost, st));
       VSAV_CUDA(cudaStreamSynchronize(st));
@@ -1693,7 +1741,7 @@ class Solver : public SolverBase {
     VSAV_CUDA(cudaMemcpyAsync(&e, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     VSAV_CUDA(cudaStreamSynchronize(st));
     s.err_flags = e;
-    if (g.nd == 2) {
+    if (bst) {                                             // a Krylov psi solve exists (2D, or 3D variable mobility)
       int S = 3 * dm.R;
       std::vector<BiState> hb(S);
       VSAV_CUDA(cudaMemcpyAsync(hb.data(), bst, S * sizeof(BiState), cudaMemcpyDeviceToHost, st));

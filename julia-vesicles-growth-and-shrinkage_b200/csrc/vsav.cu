@@ -77,6 +77,7 @@ void vsav_default_options(vsav_options* o, const vsav_config* cfg) {
   o->run_sizes = nullptr;
   o->device = 0;
   o->graph = 1;
+  o->psi3d_variable = 0;
 }
 
 int vsav_create(const vsav_config* cfg, const vsav_options* opt, vsav_handle** out) {
@@ -124,6 +125,12 @@ int vsav_create(const vsav_config* cfg, const vsav_options* opt, vsav_handle** o
       throw std::runtime_error("precision must be VSAV_FP64, VSAV_FP32 or VSAV_MIXED");
     so.psi_mixed = (o.precision == VSAV_MIXED && cfg->ndim == 2) ? 1 : 0;
     so.graph = o.graph ? 1 : 0;
+    so.psi3d_var = (cfg->ndim == 3 && o.psi3d_variable) ? 1 : 0;
+    if (so.psi3d_var) {
+      if (o.psi_form != VSAV_PSI_FULL) throw std::runtime_error("the 3D variable-mobility psi solve uses the full-spectrum form");
+      if (o.psi_precond != 0) throw std::runtime_error("the 3D variable-mobility psi solve uses the diagonal preconditioner (psi_precond 0)");
+      if (cfg->Nx > CH) throw std::runtime_error("Nx too large for the full-spectrum psi form");
+    }
     if (o.precision == VSAV_FP32)
       h->s = new Solver<float>(d, p, so, rs.data(), cfg->psi_in_v, cfg->psi_out_v);
     else
@@ -279,7 +286,7 @@ int vsav_get_work(vsav_handle* h, int32_t what, int32_t idx, double* out) {
 }
 int vsav_get_scalar_work(vsav_handle* h, int32_t what, double* out) {
   return guard(h, [&] {
-    if (!out || what < 0 || what > 5 || (what == 5 && h->nd != 2)) throw std::runtime_error("bad scalar work id");
+    if (!out || what < 0 || what > 5) throw std::runtime_error("bad scalar work id");
     h->s->get_scalar_work(what, out);
     return VSAV_OK;
   });

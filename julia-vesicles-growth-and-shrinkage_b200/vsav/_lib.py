@@ -48,7 +48,7 @@ class VsavOptions(ct.Structure):
     _fields_ = [("precision", ct.c_int32), ("psi_form", ct.c_int32), ("psi_precond", ct.c_int32),
                 ("psi_itmax", ct.c_int32), ("psi_rtol", ct.c_double), ("psi_atol", ct.c_double),
                 ("n_runs", ct.c_int32), ("run_sizes", ct.POINTER(ct.c_int32)), ("device", ct.c_int32),
-                ("graph", ct.c_int32)]
+                ("graph", ct.c_int32), ("psi3d_variable", ct.c_int32)]
 
 
 class VsavShape2D(ct.Structure):

@@ -35,14 +35,16 @@ class Handle:
     def __init__(self, cfg, precision: str = "fp64", psi_form: Optional[str] = None,
                  run_sizes: Optional[Sequence[int]] = None, psi_itmax: int = 20,
                  psi_rtol: Optional[float] = None, psi_atol: float = 1e-14, device: int = 0,
-                 psi_precond: str = "diag", psi_net=None, graph: bool = True):
+                 psi_precond: str = "diag", psi_net=None, graph: bool = True, psi3d_variable: bool = False):
         """cfg: any object with the reference Config fields (Types.jl:27-74);
         psi_in_v / psi_out_v hold one value per vesicle field of all runs.
         psi_precond: "diag" (the reference's left-preconditioned BiCGSTAB),
         "flex_diag" / "learned" (flexible right-preconditioned BiCGSTAB with the
         diagonal, or the diagonal plus the learned correction whose parameters
         psi_net gives: an array of 7409 values or a path to an .npz with
-        "theta")."""
+        "theta").  psi3d_variable: 3D Step 1 with the 2D scheme's variable psi
+        mobility and BiCGSTAB instead of the reference's constant-mobility
+        spectral division."""
         self.lib = L.load()
         self.nd = 3 if getattr(cfg, "Nz", 0) else 2
         self.Nx, self.Ny = int(cfg.Nx), int(cfg.Ny)
@@ -72,6 +74,7 @@ class Handle:
         o.psi_form = PSI_FORM[self.psi_form]
         o.psi_precond = PSI_PRECOND[psi_precond]
         o.graph = 1 if graph else 0
+        o.psi3d_variable = 1 if psi3d_variable else 0
         self.psi_precond = psi_precond
         o.psi_itmax = psi_itmax
         o.psi_rtol = cfg.tol if psi_rtol is None else psi_rtol

@@ -568,13 +568,17 @@ class Oracle:
     reference uses atol=1e-14, rtol=cfg.tol, itmax=20)."""
 
     def __init__(self, cfg: Config, psi_atol=1e-14, psi_rtol=None, psi_itmax=20,
-                 counter: Optional[OpCounter] = None, workers: Optional[int] = None):
+                 counter: Optional[OpCounter] = None, workers: Optional[int] = None,
+                 psi3d_variable: bool = False):
         self.cfg = cfg
         self.ops = build_operators(cfg, counter, workers)
         self.psi_atol = psi_atol
         self.psi_rtol = cfg.tol if psi_rtol is None else psi_rtol
         self.psi_itmax = psi_itmax
         self.last_psi_stats = []
+        # 3D with the 2D scheme's variable mobility M_psi(phi*) and its BiCGSTAB
+        # (an extension: Solvers_3d.jl:28-30 use the constant M0_psi)
+        self.psi3d_variable = psi3d_variable
 
     @property
     def counter(self):
@@ -675,8 +679,44 @@ class Oracle:
         cache["nu_21"] = L_psi * cache.psi_21
         return cache
 
+    def _psi_solver_3d(self, M_psi, a_dt):
+        """The 2D psi solve (Solvers.jl:39-81) restated on 3D full spectra:
+        A x = a_dt x - sum_d D1_full[d] F(M_psi F^-1(D1_full[d] S4 x)), d = x, y, z,
+        diagonal preconditioner 1/(a_dt - M_max S4 Laplacian_full), Krylov.jl
+        BiCGSTAB, solution truncated to the half spectrum."""
+        cfg, ops = self.cfg, self.ops
+        D1f = ops.D1_full
+        L_psi = cfg.S4
+        M_max = float(np.max(M_psi))
+        P_inv_diag = 1.0 / (a_dt - M_max * ops.Laplacian_full * L_psi)
+        shp = (cfg.N,) + cfg.shape
+        nkx = cfg.Nx // 2 + 1
+
+        def A_psi(xv):
+            x = xv.reshape(shp)
+            b1 = L_psi * x
+            acc = 0
+            for d in range(3):
+                acc = acc + D1f[d] * ops.fft(M_psi * ops.ifft(D1f[d] * b1))
+            return (a_dt * x - acc).reshape(-1)
+
+        def prec(rv):
+            return (rv.reshape(shp) * P_inv_diag).reshape(-1)
+
+        def solve(rhs_rhat):
+            rhs_full = ops.fft(ops.irfft(rhs_rhat))
+            sol, st = bicgstab(A_psi, rhs_full.reshape(-1), M=prec, atol=self.psi_atol,
+                               rtol=self.psi_rtol, itmax=self.psi_itmax)
+            self.last_psi_stats.append(st)
+            ops.counter.psi_iters.append(st.niter)
+            ops.counter.psi_solved.append(st.solved)
+            return sol.reshape(shp)[..., :nkx].copy()
+        return solve
+
     def _solve_step1_3d(self, present, old, bdf):
-        """Solvers_3d.jl:14-92: psi by spectral division with constant M0_psi."""
+        """Solvers_3d.jl:14-92: psi by spectral division with constant M0_psi;
+        with psi3d_variable, the 2D scheme's M_psi(phi*) (Utils_3d.jl:20) and
+        its BiCGSTAB (Solvers.jl:26-81) instead."""
         cfg, ops = self.cfg, self.ops
         dt = present.dt
         a, b, c = bdf.a, bdf.b, bdf.c
@@ -687,15 +727,23 @@ class Oracle:
         psi_star_hat = 2.0 * present.psi_hat - old.psi_hat
         L_phi = cfg.S1 * ops.Biharmonic - cfg.S2 * ops.Laplacian + cfg.S3
         L_psi = cfg.S4
-        M_psi = cfg.M0_psi
         lhs_phi = (a / dt) + cfg.M_phi * L_phi
-        lhs_psi = (a / dt) - cfg.M0_psi * L_psi * ops.Laplacian
+        if self.psi3d_variable:
+            M_psi = get_M_psi(phi_star, cfg)
+            self.last_psi_stats = []
+            psi_div = self._psi_solver_3d(M_psi, a / dt)
+        else:
+            M_psi = cfg.M0_psi
+            lhs_psi = (a / dt) - cfg.M0_psi * L_psi * ops.Laplacian
+
+            def psi_div(rh):
+                return rh / lhs_psi
         cache = Step1Cache()
         rh = -(b * present.phi_hat + c * old.phi_hat) / dt
         cache["phi_11"] = rh / lhs_phi
         cache["mu_11"] = L_phi * cache.phi_11
         rh = -(b * present.psi_hat + c * old.psi_hat) / dt
-        cache["psi_11"] = rh / lhs_psi
+        cache["psi_11"] = psi_div(rh)
         cache["nu_11"] = L_psi * cache.psi_11
         H1h = ops.rfft(get_H1(phi_star, ops, cfg, A0))
         cache["phi_12"] = (-cfg.M_phi * H1h) / lhs_phi
@@ -704,7 +752,7 @@ class Oracle:
         gG = [ops.irfft(ops.D1[d] * Gh) for d in range(3)]
         tc = [ops.rfft(M_psi * gG[d]) for d in range(3)]
         rh = ops.D1[0] * tc[0] + ops.D1[1] * tc[1] + ops.D1[2] * tc[2]
-        cache["psi_12"] = rh / lhs_psi
+        cache["psi_12"] = psi_div(rh)
         cache["nu_12"] = L_psi * cache.psi_12 + Gh
         H2h = ops.rfft(get_H2(phi_star, ops, cfg))
         H3h = ops.rfft(get_H3(phi_star, psi_star, cfg))
@@ -721,7 +769,7 @@ class Oracle:
         gr = [ops.irfft(ops.D1[d] * psi_star_hat) for d in range(3)]
         t = u_star[0] * gr[0] + u_star[1] * gr[1] + u_star[2] * gr[2]
         th = ops.rfft(t)
-        cache["psi_21"] = (-th) / lhs_psi
+        cache["psi_21"] = psi_div(-th)
         cache["nu_21"] = L_psi * cache.psi_21
         return cache
 
