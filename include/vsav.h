@@ -105,6 +105,19 @@ void vsav_default_options(vsav_options* opt, const vsav_config* cfg);
 /* FieldState upload/download (Types.jl:167-201), level VSAV_PRESENT / VSAV_OLD */
 int vsav_set_field(vsav_handle* h, int32_t level, int32_t field, const double* data);
 int vsav_get_field(vsav_handle* h, int32_t level, int32_t field, double* data);
+
+/* Float32 frames for headless visualisation (the arrays scripts/visualize.jl
+ * plots; no counterpart in the C sense -- the reference draws them with
+ * CairoMakie):  VSAV_EXPORT_PHI_SUM, per run, the sum of its vesicle fields
+ * + N - 1 (the phi_plot of simulation.jl:124 / Main.jl:119), [R][Nz][Ny][Nx];
+ * VSAV_EXPORT_SPEED, per run, |u| (visualize.jl:71-73); VSAV_EXPORT_FIELD +
+ * a physical field id (VSAV_PHI, VSAV_PSI, VSAV_U, VSAV_P, VSAV_MU, VSAV_NU), the
+ * field as float32 in vsav_get_field's layout.  Computed and narrowed on the
+ * device; only float32 crosses to the host. */
+#define VSAV_EXPORT_PHI_SUM 0
+#define VSAV_EXPORT_SPEED 1
+#define VSAV_EXPORT_FIELD 100
+int vsav_export_f32(vsav_handle* h, int32_t level, int32_t what, float* data);
 /* scalars Q, R1, R2, R3 per run: q4[R][4] */
 int vsav_set_scalars(vsav_handle* h, int32_t level, const double* q4);
 int vsav_get_scalars(vsav_handle* h, int32_t level, double* q4);

@@ -50,6 +50,8 @@ class SolverBase {
   virtual ~SolverBase() {}
   virtual void set_field(int level, int fid, const void* host, int is_device) = 0;
   virtual void get_field(int level, int fid, void* host) = 0;
+  // float32 frames for headless visualisation (what: 0 phi sum per run, 1 speed per run, 100 + field id)
+  virtual void export_f32(int level, int what, float* host) = 0;
   virtual void set_scalars(int level, const double* q4 /* [R][4] Q,R1,R2,R3 */) = 0;
   virtual void get_scalars(int level, double* q4) = 0;
   virtual void set_dt(const double* dt) = 0;
@@ -254,6 +256,35 @@ __global__ void k_shapes2d(T* __restrict__ phi, T* __restrict__ psi, const Shape
     phi[k] = (T)p;
     psi[k] = (T)(s.psi_in * (1 + p) / 2 + s.psi_out * (1 - p) / 2);
   }
+}
+
+// Frames for headless visualisation, as float32 (the arrays the reference's plots
+// draw, scripts/visualize.jl): per run r, phi_plot = sum of the run's vesicle
+// fields + N_r - 1 (simulation.jl:124, Main.jl:119), or the speed |u|
+// (visualize.jl:71-73).  out: [R][P].
+template <typename T>
+__global__ void k_export_run(const T* __restrict__ phi, const T* __restrict__ u, const int* __restrict__ vbeg, int what,
+                             int R, int nd, long long P, float* __restrict__ out) {
+  const long long tot = (long long)R * P;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < tot; k += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(k / P);
+    const long long q = k - (long long)r * P;
+    double s = 0.0;
+    if (what == 0) {
+      const int v0 = vbeg[r], v1 = vbeg[r + 1];
+      for (int v = v0; v < v1; ++v) s += (double)phi[(long long)v * P + q];
+      s += (double)(v1 - v0) - 1.0;
+    } else {
+      for (int d = 0; d < nd; ++d) { const double c = (double)u[((long long)d * R + r) * P + q]; s += c * c; }
+      s = sqrt(s);
+    }
+    out[k] = (float)s;
+  }
+}
+template <typename T>
+__global__ void k_to_f32(const T* __restrict__ in, float* __restrict__ out, long long n) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    out[k] = (float)in[k];
 }
 
 // One vesicle field of the reference's generate_initial_condition (Init.jl:74-197,
@@ -1639,6 +1670,38 @@ class Solver : public SolverBase {
   }
   void set_field(int level, int fid, const void* host, int is_device) override { xfer(level, fid, (void*)host, 0, is_device); }
   void get_field(int level, int fid, void* host) override { xfer(level, fid, host, 1); }
+  void export_f32(int level, int what, float* host) override {
+    const int V = dm.V, R = dm.R, nd = g.nd;
+    const long long VP = (long long)V * g.P, RP = (long long)R * g.P;
+    float* out = reinterpret_cast<float*>(stage);
+    long long n = RP;
+    const T* src = nullptr;
+    if (what != 0 && what != 1) {
+      switch (what - 100) {
+        case F_PHI: src = phys4[level]; n = VP; break;
+        case F_PSI: src = phys4[level] + VP; n = VP; break;
+        case F_MU: src = phys4[level] + 2 * VP; n = VP; break;
+        case F_NU: src = phys4[level] + 3 * VP; n = VP; break;
+        case F_U: src = uphys[level]; n = nd * RP; break;          // [nd][R][P] on the device
+        case F_P: src = uphys[level] + nd * RP; n = RP; break;
+        default: throw std::runtime_error("export: physical-space fields only");
+      }
+    }
+    if ((size_t)n * sizeof(float) > stage_bytes) throw std::runtime_error("export larger than the staging buffer");
+    if (src) { k_to_f32<T><<<gridfor(n), 256, 0, st>>>(src, out, n); VSAV_COUNT_LAUNCH(); }
+    else { k_export_run<T><<<gridfor(n), 256, 0, st>>>(phys4[level], uphys[level], d_vbeg, what, R, nd, g.P, out); VSAV_COUNT_LAUNCH(); }
+    VSAV_LAUNCH_CHECK();
+    if (what == 100 + F_U && R > 1) {
+      // host order [R][nd][P] (vsav_get_field's), one copy per (run, component)
+      for (int r = 0; r < R; ++r)
+        for (int d = 0; d < nd; ++d)
+          VSAV_CUDA(cudaMemcpyAsync(host + ((long long)r * nd + d) * g.P, out + ((long long)d * R + r) * g.P,
+                                    g.P * sizeof(float), cudaMemcpyDeviceToHost, st));
+    } else {
+      VSAV_CUDA(cudaMemcpyAsync(host, out, n * sizeof(float), cudaMemcpyDeviceToHost, st));
+    }
+    VSAV_CUDA(cudaStreamSynchronize(st));
+  }
   void set_scalars(int level, const double* q4) override {
     VSAV_CUDA(cudaMemcpyAsync(sc[level], q4, 4 * dm.R * sizeof(double), cudaMemcpyHostToDevice, st));
     VSAV_CUDA(cudaStreamSynchronize(st));

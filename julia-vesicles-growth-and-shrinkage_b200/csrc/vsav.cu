@@ -171,6 +171,15 @@ int vsav_get_field(vsav_handle* h, int32_t level, int32_t field, double* data) {
     return VSAV_OK;
   });
 }
+int vsav_export_f32(vsav_handle* h, int32_t level, int32_t what, float* data) {
+  return guard(h, [&] {
+    const bool ok = what == VSAV_EXPORT_PHI_SUM || what == VSAV_EXPORT_SPEED ||
+                    (what >= VSAV_EXPORT_FIELD && what <= VSAV_EXPORT_FIELD + VSAV_NU_HAT && (what - VSAV_EXPORT_FIELD) % 2 == 0);
+    if ((level != 0 && level != 1) || !ok || !data) throw std::runtime_error("bad export id/level");
+    h->s->export_f32(level, what, data);
+    return VSAV_OK;
+  });
+}
 int vsav_set_scalars(vsav_handle* h, int32_t level, const double* q4) {
   return guard(h, [&] { if (!q4 || (level != 0 && level != 1)) throw std::runtime_error("bad args"); h->s->set_scalars(level, q4); return VSAV_OK; });
 }

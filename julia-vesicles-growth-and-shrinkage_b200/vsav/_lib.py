@@ -19,7 +19,7 @@ FIELD_ID = {k: i for i, k in enumerate(FIELDS)}
 
 # every function declared in include/vsav.h
 EXPORTS = ("vsav_create", "vsav_destroy", "vsav_last_error", "vsav_create_error", "vsav_default_options",
-           "vsav_set_field", "vsav_get_field", "vsav_set_scalars", "vsav_get_scalars", "vsav_set_dt",
+           "vsav_set_field", "vsav_get_field", "vsav_export_f32", "vsav_set_scalars", "vsav_get_scalars", "vsav_set_dt",
            "vsav_get_dt", "vsav_set_A0", "vsav_get_A0", "vsav_init_state", "vsav_init_shapes2d", "vsav_generate_initial_condition", "vsav_step1", "vsav_step2", "vsav_step3",
            "vsav_step4", "vsav_step5", "vsav_step6", "vsav_step7", "vsav_update_state", "vsav_run",
            "vsav_monitor", "vsav_get_work", "vsav_get_scalar_work", "vsav_transform", "vsav_time_run",
@@ -86,6 +86,7 @@ def load(path: str = LIB_PATH):
         "vsav_default_options": ([ct.POINTER(VsavOptions), ct.POINTER(VsavConfig)], None),
         "vsav_set_field": ([H, i32, i32, D], ct.c_int),
         "vsav_get_field": ([H, i32, i32, D], ct.c_int),
+        "vsav_export_f32": ([H, ct.c_int32, ct.c_int32, ct.POINTER(ct.c_float)], ct.c_int),
         "vsav_set_scalars": ([H, i32, D], ct.c_int),
         "vsav_get_scalars": ([H, i32, D], ct.c_int),
         "vsav_set_dt": ([H, D], ct.c_int),

@@ -147,6 +147,21 @@ class Handle:
         self._chk(self.lib.vsav_get_field(self.h, level, L.FIELD_ID[name], L.dptr(a)))
         return a
 
+    EXPORT = {"phi_sum": 0, "speed": 1}
+
+    def export_f32(self, what: str, level: int = 0) -> np.ndarray:
+        """Float32 frame computed on the device (vsav_export_f32): "phi_sum"
+        (per run, the sum of its vesicle fields + N - 1, simulation.jl:124),
+        "speed" (per run, |u|), or a physical field name ("phi", "psi", "mu",
+        "nu", "u", "p") narrowed to float32."""
+        if what in self.EXPORT:
+            code, shape = self.EXPORT[what], (self.R,) + self.sp
+        else:
+            code, shape = 100 + L.FIELD_ID[what], self.field_shape(what)
+        a = np.empty(shape, dtype=np.float32)
+        self._chk(self.lib.vsav_export_f32(self.h, level, code, a.ctypes.data_as(ct.POINTER(ct.c_float))))
+        return a
+
     def set_scalars(self, q4, level=0):
         a = np.ascontiguousarray(np.asarray(q4, dtype=np.float64).reshape(self.R, 4))
         self._chk(self.lib.vsav_set_scalars(self.h, level, L.dptr(a)))
