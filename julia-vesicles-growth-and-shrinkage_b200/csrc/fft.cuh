@@ -453,6 +453,7 @@ struct ColArgs {
   int geo;
   int Nx, Ny, Nz, kp;
   double kxs, kys, kzs;
+  float fkxs, fkys, fkzs;   // the same in FP32 (col_mult_f)
 };
 
 template <typename C>
@@ -472,6 +473,31 @@ __device__ __forceinline__ C col_mult(const ColArgs& a, int mult, double ms, int
   }
   if (mult == M_DXZ && (int)kx == a.Nx / 2) return mk<C>(0.0, 0.0);
   return mult_value<C>(mult, kx * a.kxs, ky * a.kys, kz * a.kzs, ms);
+}
+
+// col_mult in FP32 arithmetic (the FP32 kernels): the same wavenumber decoding,
+// no FP64 conversions or products per element
+__device__ __forceinline__ int kfreq_i(int j, int n) { return (j < n / 2) ? j : j - n; }
+__device__ __forceinline__ cplx<float> col_mult_f(const ColArgs& a, int mult, float ms, int c, int e, long long o) {
+  int kx, ky, kz = 0;
+  switch (a.geo) {
+    case 0: kx = c; ky = kfreq_i(e, a.Ny); break;
+    case 1: kx = c % a.kp; ky = kfreq_i(c / a.kp, a.Ny); kz = kfreq_i(e, a.Nz); break;
+    case 2: kx = c; ky = kfreq_i(e, a.Ny); kz = kfreq_i((int)(o % a.Nz), a.Nz); break;
+    case 4: { const int cx = c & (a.Nx - 1); kx = (mult == M_DX0) ? kfreq_i(cx, a.Nx) : cx; ky = kfreq_i(c / a.Nx, a.Ny); kz = kfreq_i(e, a.Nz); break; }
+    case 5: kx = (mult == M_DX0) ? kfreq_i(c, a.Nx) : c; ky = kfreq_i(e, a.Ny); kz = kfreq_i((int)(o % a.Nz), a.Nz); break;
+    default: kx = (mult == M_DX0) ? kfreq_i(c, a.Nx) : c; ky = kfreq_i(e, a.Ny); break;
+  }
+  if (mult == M_DXZ && kx == a.Nx / 2) return mk<cplx<float>>(0.0, 0.0);
+  const float fx = (float)kx * a.fkxs, fy = (float)ky * a.fkys, fz = (float)kz * a.fkzs;
+  switch (mult) {
+    case M_DX: case M_DX0: case M_DXZ: return cplx<float>{0.f, ms * fx};
+    case M_DY: return cplx<float>{0.f, ms * fy};
+    case M_DZ: return cplx<float>{0.f, ms * fz};
+    case M_LAP: return cplx<float>{-ms * (fx * fx + fy * fy + fz * fz), 0.f};
+    case M_BIH: { const float k2 = fx * fx + fy * fy + fz * fz; return cplx<float>{ms * k2 * k2, 0.f}; }
+    default: return cplx<float>{ms, 0.f};
+  }
 }
 
 template <typename T, int E, int NT, bool INV>
@@ -505,7 +531,10 @@ __global__ void __launch_bounds__(NT, MinB<E, NT>::v) k_cols(const cplx<T>* __re
 #pragma unroll
     for (int j = 0; j < E; ++j) {
       if (!in1 && a0 != (T)1) { v[j].x *= a0; v[j].y *= a0; }
-      if (mult != M_ONE) v[j] = v[j] * col_mult<C>(a, mult, mscale, c, i + j * LE, o);
+      if (mult != M_ONE) {
+        if constexpr (std::is_same<T, float>::value) v[j] = v[j] * col_mult_f(a, mult, (float)mscale, c, i + j * LE, o);
+        else v[j] = v[j] * col_mult<C>(a, mult, mscale, c, i + j * LE, o);
+      }
     }
   } else {
 #pragma unroll

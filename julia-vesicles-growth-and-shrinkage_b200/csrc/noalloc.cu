@@ -106,6 +106,7 @@ extern "C" int vsav_irfft2d_f32_noalloc(const float* spec, float* out, int32_t n
   ColArgs a{};
   a.geo = 0; a.Nx = Nx; a.Ny = Ny; a.Nz = 1; a.kp = nkx;
   a.kxs = 2 * M_PI / Lx; a.kys = 2 * M_PI / Ly; a.kzs = 0.0;
+  a.fkxs = (float)a.kxs; a.fkys = (float)a.kys; a.fkzs = 0.f;
   a.logL = ilog2i(Ny); a.S = nkx; a.W = nkx; a.O = (long long)Ny * nkx; a.kpv = nkx; a.nkv = nkx;
   int TW = std::max(1, E * NT / Ny);
   while (TW > 1 && TW / 2 >= a.W) TW /= 2;

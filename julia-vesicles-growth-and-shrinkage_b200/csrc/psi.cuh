@@ -281,6 +281,11 @@ __global__ void __launch_bounds__(NT, MinB<E, NT>::v) k_psi_cols_inv2(const cplx
 #pragma unroll
     for (int j = 0; j < E; ++j) xr[j] = valid ? xin[(long long)(i + j * LE) * a.S] : mk<C>(0.0, 0.0);
   }
+  // FP32: the multipliers i kx0 S4 (per column) and i ky S4 (per element) in FP32 arithmetic,
+  // ky from the element's row e = i + j L/E without integer conversions in the loop
+  constexpr bool F32 = std::is_same<T, float>::value;
+  const float fkx = F32 ? (float)(kfreq(c, a.Nx) * a.kxs * S4) : 0.f, fky = F32 ? (float)(a.kys * S4) : 0.f;
+  const float fi = (float)i, fLE = (float)LE, fNy = (float)a.Ny;
 #pragma unroll 1
   for (int d = 0; d < 2; ++d) {
     const int mult = d == 0 ? M_DX0 : M_DY;
@@ -291,7 +296,17 @@ __global__ void __launch_bounds__(NT, MinB<E, NT>::v) k_psi_cols_inv2(const cplx
         C xv;
         if constexpr (E <= 8) xv = xr[j];
         else xv = xin[(long long)(i + j * LE) * a.S];
-        v[j] = xv * col_mult<C>(a, mult, S4, c, i + j * LE, 0);
+        if constexpr (F32) {
+          float k = fkx;
+          if (d == 1) {
+            float ke = fmaf((float)j, fLE, fi);
+            if (i + j * LE >= (a.Ny >> 1)) ke -= fNy;
+            k = ke * fky;
+          }
+          v[j] = mk<C>(-k * xv.y, k * xv.x);
+        } else {
+          v[j] = xv * col_mult<C>(a, mult, S4, c, i + j * LE, 0);
+        }
       }
     } else {
 #pragma unroll

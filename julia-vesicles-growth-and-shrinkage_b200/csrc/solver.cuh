@@ -666,6 +666,7 @@ class Solver : public SolverBase {
     ColArgs a{};
     a.geo = geo; a.Nx = g.Nx; a.Ny = g.Ny; a.Nz = g.Nz; a.kp = g.kp;
     a.kxs = g.kxs; a.kys = g.kys; a.kzs = g.kzs;
+    a.fkxs = (float)g.kxs; a.fkys = (float)g.kys; a.fkzs = (float)g.kzs;
     int L;
     if (geo == 0) { L = g.Ny; a.S = g.kp; a.W = g.kp; a.O = (long long)g.Ny * g.kp; a.kpv = g.kp; a.nkv = g.nkx; }
     else if (geo == 1) { L = g.Nz; a.S = g.Ny * g.kp; a.W = g.Ny * g.kp; a.O = g.H; a.kpv = g.kp; a.nkv = g.nkx; }

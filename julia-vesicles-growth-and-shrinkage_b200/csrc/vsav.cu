@@ -248,12 +248,20 @@ int vsav_run(vsav_handle* h, int32_t n0, int32_t nsteps, const double* dt, doubl
     int worst = VSAV_OK;
     std::vector<double> e(h->R), a(h->R);
     const bool mon = energy || area_ratio;
+    // st reports the first step whose psi solve did not converge, else the last step
+    vsav_status cur{}, first_bad{};
+    bool bad = false;
+    auto note = [&](int rc) {
+      if (rc > 0 && !bad) { first_bad = cur; bad = true; }
+      if (st) *st = bad ? first_bad : cur;
+    };
     for (int k = 0; k < nsteps; ++k) {
       if (dt) h->s->set_dt(dt + (size_t)k * h->R);
       int n = n0 + k;
       // whole step from a CUDA graph (errors of the step are read after it)
       if (h->s->step_graph(n, mon ? e.data() : nullptr, mon ? a.data() : nullptr)) {
-        int rc = check_status(h, st);
+        int rc = check_status(h, &cur);
+        note(rc);
         if (rc < 0) return rc;
         if (rc > 0) worst = rc;
         for (int r = 0; r < h->R; ++r) {
@@ -263,7 +271,8 @@ int vsav_run(vsav_handle* h, int32_t n0, int32_t nsteps, const double* dt, doubl
         continue;
       }
       h->s->step1(n);
-      int rc = check_status(h, st);
+      int rc = check_status(h, &cur);
+      note(rc);
       if (rc < 0) return rc;
       if (rc > 0) worst = rc;
       h->s->step2(n); h->s->step3(); h->s->step4(n); h->s->step5(n); h->s->step6(); h->s->step7(n);

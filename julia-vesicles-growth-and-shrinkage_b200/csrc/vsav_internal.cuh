@@ -10,6 +10,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <type_traits>
 #include <cstdio>
 #include <cmath>
 #include <string>

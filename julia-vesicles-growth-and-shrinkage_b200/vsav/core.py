@@ -273,7 +273,12 @@ class Handle:
     def time_run(self, n0, nsteps, monitor=True):
         """nsteps full steps timed on the device with CUDA events (ms)."""
         ms = np.zeros(1)
-        self._chk(self.lib.vsav_time_run(self.h, n0, nsteps, None, int(monitor), L.dptr(ms)))
+        rc = self.lib.vsav_time_run(self.h, n0, nsteps, None, int(monitor), L.dptr(ms))
+        if rc == L.VSAV_W_NOT_CONVERGED:
+            warnings.warn(f"BiCGSTAB did not converge in at least one of the {nsteps} timed steps",
+                          NotConvergedWarning, stacklevel=2)
+        else:
+            self._chk(rc)
         return float(ms[0])
 
     KCLASS = ("fft_cols", "fft_rows_r2c", "fft_rows_c2r", "fft_rows_c2c", "psi_rows_fused", "psi_combine",

@@ -165,12 +165,16 @@ def test_ensemble_runs_are_independent(prec):
     he = make(kwe, run_sizes=[1, 2], precision=prec)
     he.init_state(np.concatenate([phia, phib]), np.concatenate([psia, psib]))
     Ee, _ = he.run(1, 3, monitor=True)
+    # mixed: the two handles' FP32 inner sweeps differ in rounding (autotuned FFT variants of
+    # different batch sizes); the FP64 refinement brings psi to conf.tol = 1e-12, and u, driven
+    # by the amplified mu, agrees to a few 1e-12
+    tol_u = 1e-12 if prec == "fp64" else 1e-11
     for r, (kw, phi, psi, sl) in enumerate(((kwa, phia, psia, slice(0, 1)), (kwb, phib, psib, slice(1, 3)))):
         h = make(kw, precision=prec)
         h.init_state(phi, psi)
         E, _ = h.run(1, 3, monitor=True)
         assert rel(he.get_field("phi")[sl], h.get_field("phi")) < 1e-12
-        assert rel(he.get_field("u")[r], h.get_field("u")[0]) < 1e-12
+        assert rel(he.get_field("u")[r], h.get_field("u")[0]) < tol_u
         np.testing.assert_allclose(he.get_scalars()[r], h.get_scalars()[0], rtol=1e-12)
         np.testing.assert_allclose(Ee[:, r], E[:, 0], rtol=1e-12)
         h.close()
