@@ -471,7 +471,7 @@ def run_config(args):
            "warmup": args.warmup, "dt": kw["dt"], "grid": [kw["Nx"], kw["Ny"]] + ([kw["Nz"]] if kw.get("Nz") else []),
            "vesicles": kw["N"], "psi3d_variable": variable}
     ref = None
-    for prec in ("fp64", fast):
+    for prec in ("fp64", fast) + (("mixed",) if variable else ()):
         xo = dict(psi3d_variable=True) if variable else {}
         if variable and prec == "fp32":
             # the tightest tolerance one FP32 solve reaches reliably (the mixed 2D mode's sweep floor)

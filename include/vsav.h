@@ -53,7 +53,8 @@ typedef struct vsav_config {
 
 #define VSAV_FP64 0             /* every field and transform in FP64 */
 #define VSAV_FP32 1             /* FP32 fields/FFTs; FP64 SAV inner products, 3x3 and Q solves */
-#define VSAV_MIXED 2            /* FP64 fields/FFTs; the 2D psi BiCGSTAB in FP32 with FP64 iterative refinement */
+#define VSAV_MIXED 2            /* FP64 fields/FFTs; the psi BiCGSTAB (2D, or 3D with psi3d_variable) in FP32
+                                   with FP64 iterative refinement */
 #define VSAV_PSI_FULL 0         /* psi BiCGSTAB on full complex spectra: the reference's form */
 #define VSAV_PSI_HALF 1         /* psi BiCGSTAB on half spectra of real fields (Nyquist-projected) */
 

@@ -498,7 +498,7 @@ class Solver : public SolverBase {
     d_err = dalloc<int>(1);
     if (nd == 2 || opt.psi3d_var) {
       long long n = psi_n();
-      if (nd == 3 && (!psi_full() || opt.psi_precond != 0 || opt.psi_mixed))
+      if (nd == 3 && (!psi_full() || opt.psi_precond != 0))
         throw std::runtime_error("the 3D variable-mobility psi solve is the full-spectrum, diagonal-preconditioned form");
       vb = dalloc<C>(3 * V * n); vr = dalloc<C>(3 * V * n); vp = dalloc<C>(3 * V * n);
       vv = dalloc<C>(3 * V * n); vs = dalloc<C>(3 * V * n); vt = dalloc<C>(3 * V * n);
@@ -525,7 +525,7 @@ class Solver : public SolverBase {
     VSAV_CUDA(cudaStreamSynchronize(st));
     autotune();
     if constexpr (std::is_same<T, double>::value) {
-      if (opt.psi_mixed && nd == 2) {
+      if (opt.psi_mixed && (nd == 2 || opt.psi3d_var)) {
         Options o2 = opt;
         o2.psi_mixed = 0;
         std::vector<int> rs(dm.R);

@@ -123,9 +123,11 @@ int vsav_create(const vsav_config* cfg, const vsav_options* opt, vsav_handle** o
     so.psi_itmax = o.psi_itmax; so.psi_rtol = o.psi_rtol; so.psi_atol = o.psi_atol;
     if (o.precision != VSAV_FP64 && o.precision != VSAV_FP32 && o.precision != VSAV_MIXED)
       throw std::runtime_error("precision must be VSAV_FP64, VSAV_FP32 or VSAV_MIXED");
-    so.psi_mixed = (o.precision == VSAV_MIXED && cfg->ndim == 2) ? 1 : 0;
     so.graph = o.graph ? 1 : 0;
     so.psi3d_var = (cfg->ndim == 3 && o.psi3d_variable) ? 1 : 0;
+    // mixed: the psi BiCGSTAB in FP32 inside FP64 refinement wherever there is one (2D, 3D variable
+    // mobility); otherwise (3D constant mobility) every field stays FP64
+    so.psi_mixed = (o.precision == VSAV_MIXED && (cfg->ndim == 2 || so.psi3d_var)) ? 1 : 0;
     if (so.psi3d_var) {
       if (o.psi_form != VSAV_PSI_FULL) throw std::runtime_error("the 3D variable-mobility psi solve uses the full-spectrum form");
       if (o.psi_precond != 0) throw std::runtime_error("the 3D variable-mobility psi solve uses the diagonal preconditioner (psi_precond 0)");

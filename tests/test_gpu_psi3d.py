@@ -82,6 +82,23 @@ def test_variable_mobility_3d_fp32():
     h.close()
 
 
+def test_variable_mobility_3d_mixed():
+    """FP64 fields with the 3D psi BiCGSTAB in FP32 inside FP64 refinement: at conf.tol 1e-12
+    (two FP32 sweeps of 1e-6) the fields stay at FP64 accuracy."""
+    from vsav import ics
+    kw = kw3()
+    phi, psi = ics.single3d(32, 0.2, 1)
+    pres, E, _ = oracle_run(kw, phi, psi, 3)
+    h = handle(kw, psi3d_variable=True, precision="mixed")
+    h.init_state(phi, psi)
+    Eg, _ = h.run(1, 3, monitor=True)
+    for k in FIELDS:
+        assert rel(h.get_field(k), getattr(pres, k)) < 1e-8, (k, rel(h.get_field(k), getattr(pres, k)))
+    np.testing.assert_allclose(Eg[:, 0], E, rtol=1e-9)
+    assert np.all(h.psi_stats()[:, 1] == 1)
+    h.close()
+
+
 def test_variable_mobility_3d_ensemble():
     """Two 3D runs in one handle solve their psi systems independently."""
     from vsav import ics
