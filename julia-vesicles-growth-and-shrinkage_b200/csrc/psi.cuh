@@ -67,6 +67,18 @@ __global__ void __launch_bounds__(NT, MinB<E, NT>::v) k_rows_mul(cplx<T>* __rest
   const bool act = line < rows_left;
   const RowLay lay{LP};
   C v[E];
+  // the row's M values, loaded before the inverse transform so their latency overlaps it
+  T mv[FULL ? E : 2 * E];
+  {
+    const long long prow0 = (long long)v_ * rows_per_field + (row0 % rows_per_field) + line;
+    const T* Mr0 = (M && act) ? M + prow0 * (long long)Nx : nullptr;
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int e = i + j * LE;
+      if (FULL) mv[j] = (Mr0 ? Mr0[e] : mconst) * scale;
+      else { mv[2 * j] = (Mr0 ? Mr0[2 * e] : mconst) * scale; mv[2 * j + 1] = (Mr0 ? Mr0[2 * e + 1] : mconst) * scale; }
+    }
+  }
   // inverse x transform, result in registers (element i + j L/E of the row)
   if (FULL) {
     if (act) {
@@ -80,18 +92,10 @@ __global__ void __launch_bounds__(NT, MinB<E, NT>::v) k_rows_mul(cplx<T>* __rest
   }
   // multiply by M_psi of the row's vesicle (HALF: z[m] holds x[2m] + i x[2m+1])
   if (act) {
-    const long long prow = (long long)v_ * rows_per_field + (row0 % rows_per_field) + line;
-    const T* Mr = M ? M + prow * (long long)Nx : nullptr;
 #pragma unroll
     for (int j = 0; j < E; ++j) {
-      int e = i + j * LE;
-      if (FULL) {
-        T m = (Mr ? Mr[e] : mconst) * scale;
-        v[j].x *= m; v[j].y *= m;
-      } else {
-        T m0 = (Mr ? Mr[2 * e] : mconst) * scale, m1 = (Mr ? Mr[2 * e + 1] : mconst) * scale;
-        v[j].x *= m0; v[j].y *= m1;
-      }
+      if (FULL) { v[j].x *= mv[j]; v[j].y *= mv[j]; }
+      else { v[j].x *= mv[2 * j]; v[j].y *= mv[2 * j + 1]; }
     }
   }
   __syncthreads();   // smem is reused by the forward transform
@@ -361,20 +365,9 @@ __global__ void __launch_bounds__(NT, MinB<E, NT>::v) k_psi_cols_comb(const cplx
     for (int j = 0; j < E; ++j) res[(i + j * LE) * a.TW + cl] = v[j];
 #pragma unroll
     for (int j = 0; j < E; ++j) v[j] = valid ? t1[off + (long long)(i + j * LE) * a.S] : mk<C>(0.0, 0.0);
-    // the operands of the combine, loaded while t1 is transformed (small E only: registers)
-    constexpr int EP = E <= 8 ? E : 1;
-    C xp[EP], cp[EP];
+    // x and c/s are read in the epilogue: prefetching them into registers during the t1
+    // transform measured slower (register pressure, spills) than the plain loads
     const long long gbase = (long long)f * a.O + c;
-    if constexpr (E <= 8) {
-      if (valid) {
-#pragma unroll
-        for (int j = 0; j < E; ++j) {
-          const long long idx = gbase + (long long)(i + j * LE) * a.S;
-          xp[j] = x ? x[idx] : mk<C>(0.0, 0.0);
-          cp[j] = mode == 0 ? cvec[idx] : svec[idx];
-        }
-      }
-    }
     __syncthreads();                                        // the first transform's smem reads are done
     tile_fft<E, false, true, true>(v, buf, lay, cl, i, true, a.logL, a.logTW, tab);
     if (valid) {
@@ -386,9 +379,7 @@ __global__ void __launch_bounds__(NT, MinB<E, NT>::v) k_psi_cols_comb(const cplx
         const int e = i + j * LE;
         const double kyv = kfreq(e, a.Ny) * a.kys;
         const long long idx = gbase + (long long)e * a.S;
-        C xv, cv;
-        if constexpr (E <= 8) { xv = xp[j]; cv = cp[j]; }
-        else { xv = x ? x[idx] : mk<C>(0.0, 0.0); cv = mode == 0 ? cvec[idx] : svec[idx]; }
+        const C xv = x ? x[idx] : mk<C>(0.0, 0.0), cv = mode == 0 ? cvec[idx] : svec[idx];
         const C w2 = res[e * a.TW + cl];
         const double dx = -(kxv * (double)v[j].y + kyv * (double)w2.y);
         const double dy = kxv * (double)v[j].x + kyv * (double)w2.x;
