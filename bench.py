@@ -28,6 +28,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -76,7 +77,8 @@ class ClockSampler:
     def __init__(self, gpu_index):
         self.idx = gpu_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{gpu_index}.csv")
+        # the raw samples (set VSAV_CLOCKS_DIR to keep them); the JSON line carries the summary
+        self.path = os.path.join(os.environ.get("VSAV_CLOCKS_DIR", tempfile.gettempdir()), f"vsav_clocks_rank{gpu_index}.csv")
 
     def start(self):
         try:

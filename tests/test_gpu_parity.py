@@ -206,8 +206,8 @@ def test_ensemble_3d_runs_are_independent():
     he.close()
 
 
-# FP32-bulk bars (relative L2 after the fixture's steps).  The fields the
-# north star names (phi, psi, u, the energies, R1-R3, Q) are held to 1e-5
+# FP32-bulk bars (relative L2 after the fixture's steps).  The fields of the
+# 1e-5 accuracy bar (phi, psi, u, the energies, R1-R3, Q) are held to 1e-5
 # except where the precision split itself sets the floor:
 #  * mu = L_phi phi_hat + ... amplifies the FP32 FFT round-off floor of phi_hat
 #    by L_phi(k_max)/L_phi(0) = (S1 k^4 + S3)/S3 (22x at 64^2, ~100x on the
