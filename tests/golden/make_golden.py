@@ -4,8 +4,8 @@
 
 Each fixture holds the seeded initial condition, the config keyword
 arguments, and the oracle's state after K steps (fields, SAV scalars, modified
-energy, area ratio, BiCGSTAB iteration counts).  The parity tests load them on
-the GPU box, where neither the reference nor the oracle's reruns are needed.
+energy, area ratio, BiCGSTAB iteration counts).  The GPU parity tests load them,
+so they need neither the reference nor a rerun of the oracle.
 """
 import json
 import os
