@@ -157,6 +157,36 @@ def barrier(ws):
 
 
 # --------------------------------------------------------------------- CPU
+def class_roofline(prof, nsteps, hbm, peak_kind, traffic_file=False):
+    """HBM roofline of the kernel class with the most device time in a profile
+    (CUDA events around every launch, algorithmic bytes per launch)."""
+    byte_classes = {k: v for k, v in prof.items() if k != "psi_net"}
+    dom = max(byte_classes, key=lambda k: byte_classes[k]["ms"])
+    d = prof[dom]
+    per_launch_bytes = d["bytes"] / max(d["launches"], 1)
+    per_launch_ms = d["ms"] / max(d["launches"], 1)
+    achieved = per_launch_bytes / (per_launch_ms / 1000.0) / 1e9 if per_launch_ms > 0 else 0.0
+    # DRAM bytes of one ncu-captured launch of the class (profiles/traffic.json, headline
+    # workload only), scaled by algorithmic bytes to this class's average launch
+    traffic, traffic_note = None, None
+    tr_path = os.path.join(ROOT, "profiles", "traffic.json")
+    if traffic_file and os.path.exists(tr_path):
+        try:
+            tr = json.load(open(tr_path)).get(dom)
+            if tr:
+                traffic = tr["dram_bytes"] / tr["algorithmic_bytes"] * per_launch_bytes
+                traffic_note = (f"ncu dram__bytes_read+write of one {tr['kernel']} launch ({tr['dram_bytes']:.4g} B for "
+                                f"{tr['algorithmic_bytes']:.4g} algorithmic B), scaled to the class's mean launch")
+        except Exception:
+            traffic = None
+    tot_ms = max(sum(p["ms"] for p in prof.values()), 1e-9)
+    return {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": traffic, "traffic_note": traffic_note,
+            "algorithmic_bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms,
+            "launches_per_step": d["launches"] / nsteps, "share_of_profiled_time": d["ms"] / tot_ms,
+            "classes": prof}
+
+
 def cpu_reference(steps, warmup, rank_seed=0):
     """The oracle (NumPy FP64, scipy pocketfft with all host threads) on a
     bounded sample of the workload: one of the 8 vesicle fields of the
@@ -300,31 +330,8 @@ def run_ours(args):
     prof = h.profile_read()
     h.profile("reset")
     h.close()
-    byte_classes = {k: v for k, v in prof.items() if k != "psi_net"}
-    dom = max(byte_classes, key=lambda k: byte_classes[k]["ms"])
-    d = prof[dom]
-    per_launch_bytes = d["bytes"] / max(d["launches"], 1)
-    per_launch_ms = d["ms"] / max(d["launches"], 1)
-    achieved = per_launch_bytes / (per_launch_ms / 1000.0) / 1e9 if per_launch_ms > 0 else 0.0
-    # DRAM bytes of one ncu-captured launch of the class (profiles/traffic.json),
-    # scaled by algorithmic bytes to this class's average launch
-    traffic, traffic_note = None, None
-    tr_path = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tr_path):
-        try:
-            tr = json.load(open(tr_path)).get(dom)
-            if tr:
-                traffic = tr["dram_bytes"] / tr["algorithmic_bytes"] * per_launch_bytes
-                traffic_note = (f"ncu dram__bytes_read+write of one {tr['kernel']} launch ({tr['dram_bytes']:.4g} B for "
-                                f"{tr['algorithmic_bytes']:.4g} algorithmic B), scaled to the class's mean launch")
-        except Exception:
-            traffic = None
-    tot_ms = max(sum(p["ms"] for p in prof.values()), 1e-9)
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": traffic, "traffic_note": traffic_note,
-                "algorithmic_bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms,
-                "launches_per_step": d["launches"] / args.steps, "share_of_profiled_time": d["ms"] / tot_ms,
-                "classes": prof}
+    roofline = class_roofline(prof, args.steps, hbm, peak_kind, traffic_file=True)
+
     def net_roofline(prof, nsteps, arm):
         pn = prof.get("psi_net", {})
         if not pn.get("launches"):
@@ -465,6 +472,7 @@ def run_config(args):
     from vsav import Handle, ics
     from oracle import vsav_oracle as O
     variable = args.workload.endswith("_psivar")
+    hbm, peak_kind = peaks()
     kw, phi, psi, _ = ics.workload(args.workload.replace("_psivar", ""), seed=0)
     # 2D: the headline's dt; 3D: 1e-5 (both inside the range where the oracle's modified energy decreases)
     kw["dt"] = DT if kw.get("Nz", 0) == 0 else 1e-5
@@ -487,6 +495,14 @@ def run_config(args):
                "energy_non_increasing": bool(np.all(np.diff(E[:, 0]) <= 0))}
         if variable:
             res["psi_iters_last_step"] = [int(x) for x in h.psi_stats()[:, 0]]
+        # dominant kernel class over 2 more steps (CUDA events around every launch)
+        h.profile("reset")
+        h.profile(True)
+        h.run(1 + args.warmup + args.steps, 2, monitor=True)
+        h.profile(False)
+        rf = class_roofline(h.profile_read(), 2, hbm, peak_kind)
+        rf.pop("classes")
+        res["roofline"] = rf
         h.close()
         if ref is None:
             ref = fields
