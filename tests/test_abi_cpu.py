@@ -100,6 +100,19 @@ def test_net_and_psi_entry_points_reject_bad_arguments():
     assert lib.vsav_get_dt(None, _lib.dptr(th)) == -1
 
 
+def test_initial_condition_and_export_entry_points_reject_a_null_handle():
+    import ctypes as ct
+    from vsav import _lib
+    lib = _lib.load()
+    u = np.zeros(20)
+    assert lib.vsav_generate_initial_condition(None, 1, ord("s"), None) == -1
+    assert lib.vsav_generate_initial_condition(None, 4, ord("s"), _lib.dptr(u)) == -1
+    shapes = (_lib.VsavShape2D * 1)()
+    assert lib.vsav_init_shapes2d(None, shapes) == -1
+    f = np.zeros(16, dtype=np.float32)
+    assert lib.vsav_export_f32(None, 0, 0, f.ctypes.data_as(ct.POINTER(ct.c_float))) == -1
+
+
 @pytest.mark.skipif(cuda_available(), reason="needs a machine without a CUDA device")
 def test_net_create_fails_loudly_without_gpu():
     import ctypes as ct
