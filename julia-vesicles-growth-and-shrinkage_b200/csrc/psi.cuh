@@ -455,6 +455,122 @@ __global__ void __launch_bounds__(256) k_psi_combine3(const cplx<T>* __restrict_
   block_reduce_store<4>(acc, part + ((long long)f * ew.bpf + blockIdx.x) * 4, smm);
 }
 
+// The same forward pass split in two (the autotuner picks whichever is faster):
+//  k_psi_cols_fwd2: forward y pass of t1 and t2 reduced to z = i kx0 t1^ + i ky t2^,
+//                   written over t1 (the CTA has read its tile before it writes);
+//  k_psi_combz:     y = P^-1 (a_dt x - z) with the dot products, a streaming pass.
+template <typename T, int E, int NT>
+__global__ void __launch_bounds__(NT, MinB<E, NT>::v) k_psi_cols_fwd2(cplx<T>* t1, const cplx<T>* __restrict__ t2, ColArgs a,
+                                                                   SysMap sm, const int* __restrict__ active, int f0,
+                                                                   const cplx<T>* __restrict__ tab) {
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* s = reinterpret_cast<C*>(smraw);
+  const int L = 1 << a.logL, LE = L / E;
+  const int tile = blockIdx.x % a.tiles;
+  const int fl = blockIdx.x / a.tiles;
+  if (active && !active[sm.sys(f0 + fl)]) return;          // block-uniform
+  const int cl = threadIdx.x & (a.TW - 1), i = threadIdx.x >> a.logTW, c = tile * a.TW + cl;
+  const bool valid = c < a.W;
+  const ColLay lay{a.TW, Log2<E>::v};
+  C* const buf[2] = {s, s + col_tile_elems(L, a.TW, Log2<E>::v)};
+  C* const res = s + 2 * col_tile_elems(L, a.TW, Log2<E>::v);
+  const long long off = (long long)fl * a.O + c;
+  C v[E];
+#pragma unroll
+  for (int j = 0; j < E; ++j) v[j] = valid ? t2[off + (long long)(i + j * LE) * a.S] : mk<C>(0.0, 0.0);
+  tile_fft<E, false, true, true>(v, buf, lay, cl, i, true, a.logL, a.logTW, tab);
+#pragma unroll
+  for (int j = 0; j < E; ++j) res[(i + j * LE) * a.TW + cl] = v[j];
+#pragma unroll
+  for (int j = 0; j < E; ++j) v[j] = valid ? t1[off + (long long)(i + j * LE) * a.S] : mk<C>(0.0, 0.0);
+  __syncthreads();                                          // the first transform's smem reads are done
+  tile_fft<E, false, true, true>(v, buf, lay, cl, i, true, a.logL, a.logTW, tab);
+  if (!valid) return;
+  if constexpr (std::is_same<T, float>::value) {
+    const float kxv = (float)(kfreq(c, a.Nx) * a.kxs), fky = (float)a.kys;
+    const float fi = (float)i, fLE = (float)LE, fNy = (float)a.Ny;
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int e = i + j * LE;
+      float ke = fmaf((float)j, fLE, fi);
+      if (e >= (a.Ny >> 1)) ke -= fNy;
+      const float kyv = ke * fky;
+      const C w2 = res[e * a.TW + cl];
+      t1[off + (long long)e * a.S] = mk<C>(-(kxv * v[j].y + kyv * w2.y), kxv * v[j].x + kyv * w2.x);
+    }
+  } else {
+    const double kxv = kfreq(c, a.Nx) * a.kxs;
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int e = i + j * LE;
+      const double kyv = kfreq(e, a.Ny) * a.kys;
+      const C w2 = res[e * a.TW + cl];
+      t1[off + (long long)e * a.S] = mk<C>(-(kxv * (double)v[j].y + kyv * (double)w2.y),
+                                           kxv * (double)v[j].x + kyv * (double)w2.x);
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_psi_combz(const cplx<T>* __restrict__ x, const cplx<T>* __restrict__ z,
+                                                   cplx<T>* __restrict__ y, const cplx<T>* __restrict__ cvec,
+                                                   const cplx<T>* __restrict__ svec, int mode,
+                                                   const double* __restrict__ adt_r, const double* __restrict__ mmax_r,
+                                                   double S4, VGeom g, SysMap sm, const int* __restrict__ active, int f0,
+                                                   EW ew, double2* part) {
+  __shared__ double smm[2 * 4 * 8];
+  KSum acc[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+  // z is chunk-local (field blockIdx.y of the chunk); x, y, c, s are global (field f0 + blockIdx.y)
+  const int f = f0 + blockIdx.y;
+  z -= ((long long)f - blockIdx.y) * g.n;
+  const int sy = sm.sys(f);
+  const int r = sm.run_of[f % sm.V];
+  if (!active || active[sy]) {
+    const double adt = adt_r[r], mm = mmax_r ? mmax_r[r] : 0.0;
+    const long long beg = (long long)blockIdx.x * ew.chunk, end = min(ew.n, beg + ew.chunk);
+    constexpr int U = 4;
+    for (long long s0 = beg + threadIdx.x; s0 < end; s0 += U * blockDim.x) {
+      cplx<T> xv[U], zv[U], cv[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const long long s = s0 + (long long)u * blockDim.x;
+        if (s < end) {
+          const long long j = (long long)f * g.n + s;
+          xv[u] = x ? x[j] : cplx<T>{};
+          zv[u] = z[j];
+          cv[u] = mode == 0 ? cvec[j] : svec[j];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const long long s = s0 + (long long)u * blockDim.x;
+        if (s >= end) break;
+        int kx, ky; double kxv, kyv, w;
+        vk(g, s, kx, ky, kxv, kyv, w);
+        double ox = adt * (double)xv[u].x - (double)zv[u].x, oy = adt * (double)xv[u].y - (double)zv[u].y;
+        if (mmax_r) {
+          const double pinv = 1.0 / (adt + mm * S4 * (kxv * kxv + kyv * kyv));
+          ox *= pinv; oy *= pinv;
+        }
+        cplx<T> ot; ot.x = ox; ot.y = oy;
+        y[(long long)f * g.n + s] = ot;
+        ox = ot.x; oy = ot.y;                               // the dots use the stored (rounded) values
+        const cplx<T> c = cv[u];
+        if (mode == 0) {
+          acc[0].add((double)c.x * ox + (double)c.y * oy);
+          acc[1].add((double)c.x * oy - (double)c.y * ox);
+        } else {
+          acc[0].add(ox * (double)c.x + oy * (double)c.y);
+          acc[1].add(ox * (double)c.y - oy * (double)c.x);
+          acc[2].add(ox * ox + oy * oy);
+        }
+      }
+    }
+  }
+  block_reduce_store<4>(acc, part + ((long long)f * ew.bpf + blockIdx.x) * 4, smm);
+}
+
 // r = M^-1 b, x = 0, p = r, dots <b, r>, ||r||^2  (Krylov.jl bicgstab initialisation)
 template <typename T>
 __global__ void __launch_bounds__(256) k_psi_init(const cplx<T>* __restrict__ b, cplx<T>* __restrict__ x, cplx<T>* __restrict__ r,

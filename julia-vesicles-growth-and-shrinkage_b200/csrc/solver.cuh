@@ -575,11 +575,14 @@ class Solver : public SolverBase {
   // FAM_COLS: column passes of half spectra; FAM_COLS_PSI: of the full-spectrum
   // psi vectors (2D, 3V or 6V fields), tuned separately
   // FAM_PSI_INV2 / FAM_PSI_COMB: the fused column passes of the FULL psi operator
-  enum Fam { FAM_R2C = 0, FAM_C2R, FAM_C2C, FAM_MUL, FAM_COLS, FAM_COLS_PSI, FAM_PSI_INV2, FAM_PSI_COMB, FAM_N };
+  // FAM_PSI_FWD2: the forward pass of the split alternative to FAM_PSI_COMB (with k_psi_combz)
+  enum Fam { FAM_R2C = 0, FAM_C2R, FAM_C2C, FAM_MUL, FAM_COLS, FAM_COLS_PSI, FAM_PSI_INV2, FAM_PSI_COMB, FAM_PSI_FWD2,
+             FAM_N };
   static constexpr int NVAR = 7;
   static constexpr int VE[2][NVAR] = {{8, 8, 16, 32, 8, 16, 32}, {4, 4, 8, 16, 4, 8, 16}};      // [T==double][variant]
   static constexpr int VNT[NVAR] = {256, 512, 256, 256, 1024, 512, 128};
-  int choice[FAM_N] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int choice[FAM_N] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  int split_comb = 0;            // 1: forward pass + combine as k_psi_cols_fwd2 + k_psi_combz (autotuned)
   bool tuned_from_cache = false;
   double tune_ms[FAM_N][NVAR] = {};
   static constexpr int DIX = std::is_same<T, double>::value ? 1 : 0;
@@ -754,6 +757,32 @@ class Solver : public SolverBase {
       prof.end(st, std::is_same<T, float>::value ? KC_COLS_F32 : KC_COLS, (double)fc * g.Pfull * 3.0 * sizeof(C));
     })
   }
+  void psi_cols_fwd2(C* t1, const C* t2, int f0, int fc, bool use_active = true) {
+    SysMap sm{dm.V, dm.R, d_run_of};
+    VSAV_DISPATCH(FAM_PSI_FWD2, {
+      long long nouter = fc;
+      ColArgs a = colargs(3, nouter, E_, NT_);
+      int L = 1 << a.logL;
+      int thr = std::max(a.TW, a.TW * L / E_);
+      size_t sm_b = (2 * (size_t)col_tile_elems(L, a.TW, ilog2(E_)) + (size_t)L * a.TW) * sizeof(C);
+      long long grid = (long long)a.tiles * fc;
+      set_smem_attr<E_, NT_>((const void*)k_psi_cols_fwd2<T, E_, NT_>, sm_b);
+      prof.begin(st);
+      k_psi_cols_fwd2<T, E_, NT_><<<(unsigned)grid, thr, sm_b, st>>>(t1, t2, a, sm, use_active ? bupd : nullptr, f0, tab);
+      VSAV_COUNT_LAUNCH();
+      VSAV_LAUNCH_CHECK();
+      prof.end(st, KC_PSI_VEC, (double)fc * g.Pfull * 3.0 * sizeof(C));
+    })
+  }
+  void psi_combz(const C* x, const C* z, C* y, int mode, const C* svec, const double* pre, int f0, int fc, const EW& e,
+                 bool use_active = true) {
+    SysMap sm{dm.V, dm.R, d_run_of};
+    prof.begin(st);
+    k_psi_combz<T><<<dim3(e.bpf, (unsigned)fc), 256, 0, st>>>(x, z, y, vb, svec, mode, d_adt, pre, ph.S4, vgeom(), sm,
+                                                               use_active ? bupd : nullptr, f0, e, part); VSAV_COUNT_LAUNCH();
+    VSAV_LAUNCH_CHECK();
+    prof.end(st, KC_PSI_VEC, (double)fc * g.Pfull * 4.0 * sizeof(C));
+  }
   // returns the number of dot partials per field (column tiles)
   int psi_cols_comb(const C* t1, const C* t2, const C* x, C* y, int mode, const C* svec, const double* pre, int f0, int fc,
                     bool use_active = true) {
@@ -788,7 +817,8 @@ class Solver : public SolverBase {
   bool variant_ok(int fam, int v) const {
     int Lr = (fam == FAM_C2C || (fam == FAM_MUL && psi_full())) ? g.Nx : g.Nx / 2;
     int Lc = (g.nd == 3) ? std::min(g.Ny, g.Nz) : g.Ny;
-    int L = (fam == FAM_COLS || fam == FAM_COLS_PSI || fam == FAM_PSI_INV2 || fam == FAM_PSI_COMB) ? Lc : Lr;
+    int L = (fam == FAM_COLS || fam == FAM_COLS_PSI || fam == FAM_PSI_INV2 || fam == FAM_PSI_COMB || fam == FAM_PSI_FWD2)
+                ? Lc : Lr;
     return vE(v) <= L && vE(v) * VNT[v] / L >= 1;
   }
   void autotune() {
@@ -801,11 +831,18 @@ class Solver : public SolverBase {
     {
       std::lock_guard<std::mutex> lk(tune_mutex());
       auto it = tune_cache().find(tune_key());
-      if (it != tune_cache().end()) { for (int f = 0; f < FAM_N; ++f) choice[f] = it->second[f]; tuned_from_cache = true; return; }
+      if (it != tune_cache().end()) {
+        for (int f = 0; f < FAM_N; ++f) choice[f] = it->second[f];
+        split_comb = it->second[FAM_N];
+        tuned_from_cache = true;
+        return;
+      }
     }
     autotune_measure();
     std::lock_guard<std::mutex> lk(tune_mutex());
-    tune_cache()[tune_key()] = std::vector<int>(choice, choice + FAM_N);
+    std::vector<int> c(choice, choice + FAM_N);
+    c.push_back(split_comb);
+    tune_cache()[tune_key()] = c;
   }
   static std::mutex& tune_mutex() { static std::mutex m; return m; }
   void autotune_measure() {
@@ -821,7 +858,8 @@ class Solver : public SolverBase {
     if (have_mul) VSAV_CUDA(cudaMemsetAsync(bupd, 0xff, 3 * dm.R * sizeof(int), st));
     for (int fam = 0; fam < FAM_N; ++fam) {
       if (fam == FAM_MUL && !have_mul) continue;
-      if ((fam == FAM_C2C || fam == FAM_COLS_PSI || fam == FAM_PSI_INV2 || fam == FAM_PSI_COMB) && !(g.nd == 2 && psi_full()))
+      if ((fam == FAM_C2C || fam == FAM_COLS_PSI || fam == FAM_PSI_INV2 || fam == FAM_PSI_COMB || fam == FAM_PSI_FWD2) &&
+          !(g.nd == 2 && psi_full()))
         continue;
       double best = 1e30;
       int bestv = 0;
@@ -838,6 +876,7 @@ class Solver : public SolverBase {
             case FAM_COLS_PSI: cols(true, 3, 3LL * V, vb, nullptr, 1, 0, M_ONE, 1, vt, 1); break;
             case FAM_PSI_INV2: psi_cols_inv2(vb, vt12, vt12 + 3LL * V * psi_n(), 0, 3 * V, false); break;
             case FAM_PSI_COMB: psi_cols_comb(vt12, vt12 + 3LL * V * psi_n(), vb, vt, 0, nullptr, nullptr, 0, 3 * V, false); break;
+            case FAM_PSI_FWD2: psi_cols_fwd2(vt12, vt12 + 3LL * V * psi_n(), 0, 3 * V, false); break;
             default: cols(false, g.nd == 2 ? 0 : 1, V, tmpH, nullptr, 1, 0, M_ONE, 1, tmpH, 1); break;
           }
         };
@@ -853,15 +892,34 @@ class Solver : public SolverBase {
       }
       choice[fam] = bestv;
     }
+    // split or fused forward pass + combine: the split pair's streaming combine timed on the same fields
+    split_comb = 0;
+    if (g.nd == 2 && psi_full() && vt12 != nullptr) {
+      const long long n = psi_n();
+      EW e = ew(n);
+      auto combz = [&]() { psi_combz(vb, vt12, vt, 0, nullptr, nullptr, 0, 3 * V, e, false); };
+      combz();
+      VSAV_CUDA(cudaEventRecord(e0, st));
+      for (int k = 0; k < 3; ++k) combz();
+      VSAV_CUDA(cudaEventRecord(e1, st));
+      VSAV_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      VSAV_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      split_ms = tune_ms[FAM_PSI_FWD2][choice[FAM_PSI_FWD2]] + ms / 3;
+      split_comb = split_ms < tune_ms[FAM_PSI_COMB][choice[FAM_PSI_COMB]];
+    }
     prof.on = was;
     if (getenv("VSAV_VERBOSE")) {
-      const char* nm[FAM_N] = {"rows_r2c", "rows_c2r", "rows_c2c", "rows_mul", "cols", "cols_psi", "psi_inv2", "psi_comb"};
+      const char* nm[FAM_N] = {"rows_r2c", "rows_c2r", "rows_c2c", "rows_mul", "cols", "cols_psi", "psi_inv2", "psi_comb",
+                               "psi_fwd2"};
       for (int f = 0; f < FAM_N; ++f) for (int v = 0; v < NVAR; ++v) if (!variant_ok(f, v)) tune_ms[f][v] = -1;
       for (int f = 0; f < FAM_N; ++f) {
         fprintf(stderr, "[vsav autotune %s] %-9s", std::is_same<T, double>::value ? "fp64" : "fp32", nm[f]);
         for (int v = 0; v < NVAR; ++v) fprintf(stderr, "  E%d/NT%d %.3f ms", vE(v), VNT[v], tune_ms[f][v]);
         fprintf(stderr, "  -> %d\n", choice[f]);
       }
+      fprintf(stderr, "[vsav autotune %s] forward pass + combine: %s (split %.3f ms)\n",
+              std::is_same<T, double>::value ? "fp64" : "fp32", split_comb ? "split" : "fused", split_ms);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -1299,6 +1357,12 @@ class Solver : public SolverBase {
   // y = P^-1 A in (+ dots), chunk by chunk: y-inverse (2 multipliers), fused
   // x pass (inverse, x M_psi, forward), y-forward, combine
   EW dot_ew{};                 // partial layout of the dots of the last matvec
+  double split_ms = 0.0;
+  // VSAV_PSI_SPLIT=0/1 overrides the autotuner's choice between the fused and the split forward pass
+  bool use_split() const {
+    if (const char* env = getenv("VSAV_PSI_SPLIT")) return atoi(env) != 0;
+    return split_comb != 0;
+  }
   bool fused_ops = true;       // FULL form: fused column passes (VSAV_PSI_FUSED=0: separate kernels)
   void matvec(const C* in, C* out, int mode, const C* svec, bool precond = true) {
     if (g.nd == 3) { matvec3(in, out, mode, svec, precond); return; }
@@ -1320,8 +1384,13 @@ class Solver : public SolverBase {
         // one read of x for both inverse passes; the forward pass carries the combine
         psi_cols_inv2(in, t1, t2, f0, fc);
         rows_mul(t1, 2LL * fc * g.Ny, full, f0, fc);
-        const int tiles = psi_cols_comb(t1, t2, in, out, mode, svec, pre, f0, fc);
-        dot_ew.bpf = tiles;
+        if (use_split()) {
+          psi_cols_fwd2(t1, t2, f0, fc);
+          psi_combz(in, t1, out, mode, svec, pre, f0, fc, e);
+        } else {
+          const int tiles = psi_cols_comb(t1, t2, in, out, mode, svec, pre, f0, fc);
+          dot_ew.bpf = tiles;
+        }
         continue;
       }
       cols(true, geo, fc, in + f0 * n, nullptr, 1, 0, full ? M_DX0 : M_DXZ, ph.S4, t1, 1);

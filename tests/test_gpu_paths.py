@@ -1,7 +1,9 @@
 """The alternative code paths selected by environment switches give the
 default path's results: the unfused psi operator (VSAV_PSI_FUSED=0), the psi
-operator in L2-sized chunks of fields (VSAV_PSI_CHUNK_MB), and eager launches
-instead of CUDA-graph replay (VSAV_GRAPH=0)."""
+operator in L2-sized chunks of fields (VSAV_PSI_CHUNK_MB), eager launches
+instead of CUDA-graph replay (VSAV_GRAPH=0), and either form of the operator's
+forward pass (VSAV_PSI_SPLIT=1: k_psi_cols_fwd2 + k_psi_combz; 0: the fused
+k_psi_cols_comb), whichever the autotuner picked."""
 import numpy as np
 import pytest
 
@@ -25,7 +27,8 @@ def run(kw, phi, psi, prec, steps=3):
 
 
 @pytest.mark.parametrize("prec", ["fp64", "mixed", "fp32"])
-@pytest.mark.parametrize("env", [("VSAV_PSI_FUSED", "0"), ("VSAV_PSI_CHUNK_MB", "1"), ("VSAV_GRAPH", "0")])
+@pytest.mark.parametrize("env", [("VSAV_PSI_FUSED", "0"), ("VSAV_PSI_CHUNK_MB", "1"), ("VSAV_GRAPH", "0"),
+                                 ("VSAV_PSI_SPLIT", "1"), ("VSAV_PSI_SPLIT", "0")])
 def test_switches_keep_the_results(prec, env, monkeypatch):
     from vsav import ics
     kw, phi, psi, _ = ics.workload("multi2d_512x4", seed=2, n_override=256, N_override=2, eps_override=0.08)
