@@ -906,7 +906,8 @@ class Solver : public SolverBase {
       float ms = 0;
       VSAV_CUDA(cudaEventElapsedTime(&ms, e0, e1));
       split_ms = tune_ms[FAM_PSI_FWD2][choice[FAM_PSI_FWD2]] + ms / 3;
-      split_comb = split_ms < tune_ms[FAM_PSI_COMB][choice[FAM_PSI_COMB]];
+      // the fused form (fewer bytes) unless the split pair is clearly faster
+      split_comb = split_ms < 0.95 * tune_ms[FAM_PSI_COMB][choice[FAM_PSI_COMB]];
     }
     prof.on = was;
     if (getenv("VSAV_VERBOSE")) {
