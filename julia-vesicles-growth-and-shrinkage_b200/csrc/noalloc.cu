@@ -29,32 +29,40 @@ static __device__ __align__(256) float2 g_noalloc_tab[2 * NOALLOC_MAX_N];
 
 namespace {
 
+// Per-device set-up record.  The table has a fixed size and never moves, and
+// callers copy the two addresses out while they hold the lock, so a first
+// call on another device (from another host thread) cannot invalidate them.
+constexpr int NOALLOC_MAX_DEVICES = 64;
 struct DevSetup {
   bool done = false;
   float2* scratch = nullptr;   // device addresses of the two arrays on this device
   float2* tab = nullptr;
 };
 std::mutex g_setup_mutex;
-std::vector<DevSetup> g_setup;
+DevSetup g_setup[NOALLOC_MAX_DEVICES];
 thread_local std::string g_noalloc_error;
 
 int fail(const std::string& m, int code) { g_noalloc_error = m; return code; }
 
 // once per device, with that device current: resolve the device addresses of
 // the file-scope arrays (a host-side use of the array names would be a host
-// stand-in, not a device address) and fill the twiddle table
-int setup_device(int dev, DevSetup*& out) {
+// stand-in, not a device address) and fill the twiddle table.  The addresses
+// are returned by value.
+int setup_device(int dev, float2*& scratch, float2*& tab) {
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
+    return fail("device ordinal " + std::to_string(dev) + " is beyond the " + std::to_string(NOALLOC_MAX_DEVICES) +
+                    " devices this entry point supports",
+                VSAV_E_INVALID);
   std::lock_guard<std::mutex> lk(g_setup_mutex);
-  if ((int)g_setup.size() <= dev) g_setup.resize(dev + 1);
   DevSetup& d = g_setup[dev];
   if (!d.done) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return fail(std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e), VSAV_E_CUDA);
-    d.scratch = (float2*)p;
+    float2* sp = (float2*)p;
     e = cudaGetSymbolAddress(&p, g_noalloc_tab);
     if (e != cudaSuccess) return fail(std::string("cudaGetSymbolAddress(twiddles): ") + cudaGetErrorString(e), VSAV_E_CUDA);
-    d.tab = (float2*)p;
+    float2* tp = (float2*)p;
     std::vector<float2> ht(2 * NOALLOC_MAX_N);
     for (int n = 1; n <= NOALLOC_MAX_N; n <<= 1)
       for (int m = 0; m < n; ++m) {
@@ -65,9 +73,12 @@ int setup_device(int dev, DevSetup*& out) {
       }
     e = cudaMemcpyToSymbol(g_noalloc_tab, ht.data(), ht.size() * sizeof(float2));
     if (e != cudaSuccess) return fail(std::string("twiddle upload: ") + cudaGetErrorString(e), VSAV_E_CUDA);
+    d.scratch = sp;
+    d.tab = tp;
     d.done = true;
   }
-  out = &d;
+  scratch = d.scratch;
+  tab = d.tab;
   return VSAV_OK;
 }
 
@@ -79,9 +90,13 @@ bool pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 
 using namespace vsav;
 
+// The two launches go through cudaLaunchKernel, whose return value is the
+// status of that launch alone: an error that the caller's earlier CUDA work
+// left pending on this thread is neither reported as ours nor cleared.
 extern "C" int vsav_irfft2d_f32_noalloc(const float* spec, float* out, int32_t nf, int32_t Nx, int32_t Ny, double Lx,
                                         double Ly, int32_t mult, void* stream) {
   constexpr int E = 8, NT = 256;
+  g_noalloc_error.clear();
   if (!spec || !out) return fail("null input or output pointer", VSAV_E_INVALID);
   if (!pow2(Nx) || Nx < 32 || Nx > NOALLOC_MAX_N || !pow2(Ny) || Ny < E || Ny > NOALLOC_MAX_N)
     return fail("Nx must be a power of two in [32, 2048] and Ny a power of two in [8, 2048]", VSAV_E_INVALID);
@@ -98,8 +113,9 @@ extern "C" int vsav_irfft2d_f32_noalloc(const float* spec, float* out, int32_t n
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(std::string("cudaGetDevice: ") + cudaGetErrorString(e), VSAV_E_CUDA);
-  DevSetup* d = nullptr;
-  int rc = setup_device(dev, d);
+  float2* scratch = nullptr;
+  float2* tab = nullptr;
+  int rc = setup_device(dev, scratch, tab);
   if (rc != VSAV_OK) return rc;
   cudaStream_t st = (cudaStream_t)stream;
   // column (y) pass: spec -> scratch, both in the caller's unpadded layout [nf][Ny][nkx]
@@ -113,11 +129,24 @@ extern "C" int vsav_irfft2d_f32_noalloc(const float* spec, float* out, int32_t n
   a.TW = TW; a.logTW = ilog2i(TW); a.tiles = (a.W + TW - 1) / TW;
   const int thr_c = std::max(TW, TW * Ny / E);
   const size_t sm_c = 2 * (size_t)col_tile_elems(Ny, TW, ilog2i(E)) * sizeof(float2);
-  if (sm_c > 48 * 1024) cudaFuncSetAttribute((const void*)k_cols<float, E, NT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_c);
-  k_cols<float, E, NT, true><<<(unsigned)((long long)a.tiles * nf), thr_c, sm_c, st>>>(
-      reinterpret_cast<const float2*>(spec), nullptr, 1.0f, 0.0f, mult, 1.0, d->scratch, 1.0f, a, d->tab);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return fail(std::string("column pass launch: ") + cudaGetErrorString(e), VSAV_E_CUDA);
+  const void* kc = (const void*)k_cols<float, E, NT, true>;
+  if (sm_c > 48 * 1024) {
+    e = cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_c);
+    if (e != cudaSuccess) return fail(std::string("column pass attribute: ") + cudaGetErrorString(e), VSAV_E_CUDA);
+  }
+  {
+    const float2* in0 = reinterpret_cast<const float2*>(spec);
+    const float2* in1 = nullptr;
+    float a0 = 1.0f, a1 = 0.0f, oscale = 1.0f;
+    int m = mult;
+    double ms = 1.0;
+    float2* o = scratch;
+    const float2* t = tab;
+    void* args[] = {(void*)&in0, (void*)&in1, (void*)&a0, (void*)&a1, (void*)&m, (void*)&ms,
+                    (void*)&o, (void*)&oscale, (void*)&a, (void*)&t};
+    e = cudaLaunchKernel(kc, dim3((unsigned)((long long)a.tiles * nf)), dim3(thr_c), args, sm_c, st);
+    if (e != cudaSuccess) return fail(std::string("column pass launch: ") + cudaGetErrorString(e), VSAV_E_CUDA);
+  }
   // row (x) pass: c2r of scratch rows (pitch nkx) -> out, scaled by 1/(Nx Ny)
   const int L = Nx / 2, logL = ilog2i(L);
   const long long nrows = (long long)nf * Ny;
@@ -125,11 +154,22 @@ extern "C" int vsav_irfft2d_f32_noalloc(const float* spec, float* out, int32_t n
   while (nl > 1 && nl / 2 >= nrows) nl /= 2;
   const int thr_r = std::max(1, nl * L / E);
   const size_t sm_r = (size_t)(2 * nl * line_pitch(L) + nl) * sizeof(float2);
-  if (sm_r > 48 * 1024) cudaFuncSetAttribute((const void*)k_rows_c2r<float, E, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_r);
-  k_rows_c2r<float, E, NT><<<(unsigned)((nrows + nl - 1) / nl), thr_r, sm_r, st>>>(
-      d->scratch, out, (float)(1.0 / ((double)Nx * Ny)), logL, ilog2i(nl), nrows, nkx, d->tab);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return fail(std::string("row pass launch: ") + cudaGetErrorString(e), VSAV_E_CUDA);
+  const void* kr = (const void*)k_rows_c2r<float, E, NT>;
+  if (sm_r > 48 * 1024) {
+    e = cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_r);
+    if (e != cudaSuccess) return fail(std::string("row pass attribute: ") + cudaGetErrorString(e), VSAV_E_CUDA);
+  }
+  {
+    const float2* in = scratch;
+    float* o = out;
+    float scale = (float)(1.0 / ((double)Nx * Ny));
+    int lL = logL, lnl = ilog2i(nl), kpv = nkx;
+    long long nr = nrows;
+    const float2* t = tab;
+    void* args[] = {(void*)&in, (void*)&o, (void*)&scale, (void*)&lL, (void*)&lnl, (void*)&nr, (void*)&kpv, (void*)&t};
+    e = cudaLaunchKernel(kr, dim3((unsigned)((nrows + nl - 1) / nl)), dim3(thr_r), args, sm_r, st);
+    if (e != cudaSuccess) return fail(std::string("row pass launch: ") + cudaGetErrorString(e), VSAV_E_CUDA);
+  }
   return VSAV_OK;
 }
 
