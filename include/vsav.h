@@ -76,6 +76,13 @@ typedef struct vsav_options {
                                    division (Solvers_3d.jl:28-30); 1: the 2D scheme's variable mobility
                                    M_psi(phi*) (Utils_3d.jl:20) and its diagonal-preconditioned BiCGSTAB
                                    (Solvers.jl:26-81) on 3D full spectra -- no counterpart in the reference */
+  int32_t psi_stop;             /* 0 (default): stop the psi BiCGSTAB on the preconditioned residual,
+                                   ||M^-1 r|| <= atol + rtol ||M^-1 b|| (Krylov.jl's left-preconditioned rule,
+                                   Solvers.jl:73-75); 1: on the true residual ||b - A x|| <= atol + rtol ||b||.
+                                   The flexible solvers (psi_precond 1, 2) always stop on the true residual */
+  int32_t psi_check;            /* 1: after every psi solve, measure ||b - A x|| / ||b|| per system in the
+                                   handle's arithmetic (FP64 for VSAV_MIXED): one more operator application
+                                   per solve; read with vsav_get_scalar_work(h, 6, out[3R]) */
 } vsav_options;
 
 /* field ids (FieldState, src/Types.jl:167-201) */
@@ -199,6 +206,16 @@ int vsav_profile(vsav_handle* h, int32_t enable);
 /* kernels launched by this library so far (all handles) */
 int64_t vsav_launch_count(void);
 int vsav_profile_read(vsav_handle* h, int32_t kclass, double* out3);
+/* The FFT kernel variant (elements per thread E, threads per CTA NT) of each
+ * pass family that this handle uses, and where the choice came from
+ * ("measured" at creation, "process": an earlier handle of the same shape,
+ * "file": the JSON file named by the environment variable VSAV_TUNE_FILE,
+ * "forced": VSAV_TUNE), as a NUL-terminated JSON object written to buf
+ * (capacity cap bytes; *needed receives the size with the NUL, buf may be
+ * NULL to query it).  Replaces FFTW's plan-time measurement (the MEASURE
+ * planning of src/SpectralUtils.jl:61-71), whose wisdom the reference does not
+ * persist either. */
+int vsav_get_tuning(vsav_handle* h, char* buf, int64_t cap, int64_t* needed);
 /* compute_modified_energy(present, old) and the area ratio (simulation.jl:146-147), per run */
 int vsav_monitor(vsav_handle* h, double* energy, double* area_ratio);
 
@@ -209,7 +226,9 @@ int vsav_monitor(vsav_handle* h, double* energy, double* area_ratio);
 int vsav_get_work(vsav_handle* h, int32_t what, int32_t idx, double* out);
 /* scalar intermediates: 0 Step 2 R values [R][6] (R11 R21 R31 R12 R22 R32),
  * 1 Q [R], 2 theta_1/theta_2 [R][2], 3 area [V], 4 M_max [R],
- * 5 psi BiCGSTAB per system [3R][4] (iters, solved, status, rnorm/eps) */
+ * 5 psi BiCGSTAB per system [3R][4] (iters, solved, status, rnorm/eps),
+ * 6 measured true relative residual ||b - A x|| / ||b|| per system [3R] of the
+ * last psi solves (vsav_options.psi_check; zeros otherwise) */
 int vsav_get_scalar_work(vsav_handle* h, int32_t what, double* out);
 
 /* to_spectral! / to_physical! (SpectralUtils.jl:132-148) on nf fields:
@@ -295,8 +314,11 @@ int vsav_psi_harvest_read(vsav_handle* h, float* out, int64_t capacity, int32_t*
  * resolves that array's device address and uploads the twiddle table
  * (synchronously), so make it before any stream capture.  All calls share the
  * array: calls that can overlap on the GPU (different streams, devices'
- * threads racing on one device) race; serialise them.  The error text of a
- * failed call is returned by vsav_noalloc_error(). */
+ * threads racing on one device) race; serialise them.  vsav_noalloc_error()
+ * returns the error text of this thread's last call (empty after a success).
+ * The return code covers this call's own launches only: an error that earlier
+ * CUDA work left pending on the calling thread is neither reported nor
+ * cleared.  Device ordinals up to 63 are supported. */
 int vsav_irfft2d_f32_noalloc(const float* spec, float* out, int32_t nf, int32_t Nx, int32_t Ny, double Lx,
                              double Ly, int32_t mult, void* stream);
 const char* vsav_noalloc_error(void);

@@ -571,7 +571,7 @@ __global__ void __launch_bounds__(256) k_psi_combz(const cplx<T>* __restrict__ x
   block_reduce_store<4>(acc, part + ((long long)f * ew.bpf + blockIdx.x) * 4, smm);
 }
 
-// r = M^-1 b, x = 0, p = r, dots <b, r>, ||r||^2  (Krylov.jl bicgstab initialisation)
+// r = M^-1 b, x = 0, p = r, dots <b, r>, ||r||^2, ||b||^2  (Krylov.jl bicgstab initialisation)
 template <typename T>
 __global__ void __launch_bounds__(256) k_psi_init(const cplx<T>* __restrict__ b, cplx<T>* __restrict__ x, cplx<T>* __restrict__ r,
                                                   cplx<T>* __restrict__ p, const double* __restrict__ adt_r,
@@ -598,6 +598,7 @@ __global__ void __launch_bounds__(256) k_psi_init(const cplx<T>* __restrict__ b,
     acc[0].add(w * ((double)bv.x * (double)rv.x + (double)bv.y * (double)rv.y));
     if (g.full) acc[1].add((double)bv.x * (double)rv.y - (double)bv.y * (double)rv.x);
     acc[2].add(w * ((double)rv.x * (double)rv.x + (double)rv.y * (double)rv.y));
+    acc[3].add(w * ((double)bv.x * (double)bv.x + (double)bv.y * (double)bv.y));   // ||b||^2: the true residual of x0 = 0
   }
   block_reduce_store<4>(acc, part + ((long long)blockIdx.y * ew.bpf + blockIdx.x) * 4, smm);
 }
@@ -619,21 +620,27 @@ __global__ void k_psi_s(const cplx<T>* __restrict__ r, const cplx<T>* __restrict
   }
 }
 
-// x = (x + alpha p) + omega s ;  r = s - omega t ; dots <c, r>, ||r||^2
+// x = (x + alpha p) + omega s ;  r = s - omega t ; dots <c, r>, ||r||^2, ||D r||^2
 // (flexible right-preconditioned form: p and shat are the preconditioned
-// directions used for x, s the unpreconditioned one used for r)
+// directions used for x, s the unpreconditioned one used for r).
+// D = a_dt + M_max S4 |k|^2 is the inverse of the diagonal preconditioner: in the
+// left-preconditioned form r = M^-1 (b - A x), so ||D r|| is the norm of the true
+// residual b - A x, at no extra pass (mmax_r == nullptr: D = 1, r is already true).
 template <typename T>
 __global__ void __launch_bounds__(256) k_psi_update(cplx<T>* __restrict__ x, cplx<T>* __restrict__ r, const cplx<T>* __restrict__ p,
                                                     const cplx<T>* __restrict__ s, const cplx<T>* __restrict__ t,
                                                     const cplx<T>* __restrict__ cvec, const BiState* __restrict__ st,
                                                     VGeom g, SysMap sm, EW ew, double2* part,
-                                                    const cplx<T>* __restrict__ shat = nullptr) {
+                                                    const cplx<T>* __restrict__ shat, const double* __restrict__ adt_r,
+                                                    const double* __restrict__ mmax_r, double S4) {
   __shared__ double smm[2 * 4 * 8];
   KSum acc[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
   const int f = blockIdx.y;
   const BiState& b = st[sm.sys(f)];
   if (b.active) {
     const double2 al = b.alpha, om = b.omega;
+    const int run = sm.run_of[f % sm.V];
+    const double adt = mmax_r ? adt_r[run] : 0.0, mm = mmax_r ? mmax_r[run] : 0.0;
     const long long beg = (long long)blockIdx.x * ew.chunk, end = min(ew.n, beg + ew.chunk);
     for (long long q = beg + threadIdx.x; q < end; q += blockDim.x) {
       int kx, ky; double kxv, kyv, w;
@@ -656,7 +663,14 @@ __global__ void __launch_bounds__(256) k_psi_update(cplx<T>* __restrict__ x, cpl
       cplx<T> c = cvec[j];
       acc[0].add(w * ((double)c.x * (double)rn.x + (double)c.y * (double)rn.y));
       if (g.full) acc[1].add((double)c.x * (double)rn.y - (double)c.y * (double)rn.x);
-      acc[2].add(w * ((double)rn.x * (double)rn.x + (double)rn.y * (double)rn.y));
+      const double rr = (double)rn.x * (double)rn.x + (double)rn.y * (double)rn.y;
+      acc[2].add(w * rr);
+      double dd = 1.0;
+      if (mmax_r) {
+        const double kxp = (!g.full && kx == g.Nx / 2) ? 0.0 : kxv;
+        dd = adt + mm * S4 * (kxp * kxp + kyv * kyv + vk_kz2(g, q));
+      }
+      acc[3].add(w * dd * dd * rr);
     }
   }
   block_reduce_store<4>(acc, part + ((long long)blockIdx.y * ew.bpf + blockIdx.x) * 4, smm);
@@ -698,14 +712,16 @@ __device__ __forceinline__ void sys_sums(const double* fd, int sy, const SysMap&
   }
 }
 
+// stop_true: stop on the true residual ||b - A x|| <= atol + rtol ||b|| (slot 3 of the
+// dots) instead of Krylov.jl's preconditioned ||M^-1 r|| <= atol + rtol ||M^-1 b|| (slot 2)
 __global__ void k_bi_init(const double* __restrict__ fd, BiState* __restrict__ st, int* __restrict__ upd, SysMap sm, int S, int F,
-                          double atol, double rtol, int itmax) {
+                          double atol, double rtol, int itmax, int stop_true) {
   int sy = blockIdx.x * blockDim.x + threadIdx.x;
   if (sy >= S) return;
   double d[4];
   sys_sums(fd, sy, sm, F, d);
   BiState b{};
-  b.rnorm = sqrt(d[2]);
+  b.rnorm = sqrt(stop_true ? d[3] : d[2]);
   b.eps = atol + rtol * b.rnorm;
   b.rho = make_double2(d[0], d[1]);
   b.alpha = b.omega = make_double2(1.0, 0.0);
@@ -735,7 +751,7 @@ __global__ void k_bi_omega(const double* __restrict__ fd, BiState* __restrict__ 
   st[sy].omega = cdiv(make_double2(d[0], d[1]), make_double2(d[2], 0.0));
 }
 __global__ void k_bi_beta(const double* __restrict__ fd, BiState* __restrict__ st, int* __restrict__ upd, SysMap sm, int S, int F,
-                          int itmax, int* __restrict__ any_active) {
+                          int itmax, int* __restrict__ any_active, int stop_true) {
   int sy = blockIdx.x * blockDim.x + threadIdx.x;
   if (sy >= S) return;
   BiState b = st[sy];
@@ -746,7 +762,7 @@ __global__ void k_bi_beta(const double* __restrict__ fd, BiState* __restrict__ s
   double2 nr = make_double2(d[0], d[1]);
   b.beta = cmul(cdiv(nr, b.rho), cdiv(b.alpha, b.omega));
   b.rho = nr;
-  b.rnorm = sqrt(d[2]);
+  b.rnorm = sqrt(stop_true ? d[3] : d[2]);
   b.iters += 1;
   bool mach = (b.rnorm + 1.0 <= 1.0);
   bool solved = (b.rnorm <= b.eps) || mach;
@@ -757,6 +773,37 @@ __global__ void k_bi_beta(const double* __restrict__ fd, BiState* __restrict__ s
   b.status = solved ? 1 : (brk ? 3 : (tired ? 2 : 0));
   st[sy] = b;
   if (b.active) atomicOr(any_active, 1);
+}
+
+// ---------------------------------------------------------------------------
+// measured true residual of a finished solve: per field ||b - Ax||^2 and ||b||^2
+// (slots 0 and 1), then per system ||b - Ax|| / ||b||
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_psi_resnorm(const cplx<T>* __restrict__ b, const cplx<T>* __restrict__ ax, VGeom g,
+                                                     EW ew, double2* part) {
+  __shared__ double smm[2 * 4 * 8];
+  KSum acc[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+  const int f = blockIdx.y;
+  const long long beg = (long long)blockIdx.x * ew.chunk, end = min(ew.n, beg + ew.chunk);
+  for (long long q = beg + threadIdx.x; q < end; q += blockDim.x) {
+    int kx, ky; double kxv, kyv, w;
+    vk(g, q, kx, ky, kxv, kyv, w);
+    if (w == 0.0) continue;
+    const long long j = (long long)f * g.n + q;
+    const cplx<T> bv = b[j], av = ax[j];
+    const double rx = (double)bv.x - (double)av.x, ry = (double)bv.y - (double)av.y;
+    acc[0].add(w * (rx * rx + ry * ry));
+    acc[1].add(w * ((double)bv.x * (double)bv.x + (double)bv.y * (double)bv.y));
+  }
+  block_reduce_store<4>(acc, part + ((long long)blockIdx.y * ew.bpf + blockIdx.x) * 4, smm);
+}
+__global__ void k_psi_true_res(const double* __restrict__ fd, double* __restrict__ out, SysMap sm, int S, int F) {
+  int sy = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sy >= S) return;
+  double d[4];
+  sys_sums(fd, sy, sm, F, d);
+  out[sy] = d[1] > 0.0 ? sqrt(d[0] / d[1]) : 0.0;
 }
 
 // ---------------------------------------------------------------------------

@@ -14,6 +14,7 @@
 #include <type_traits>
 #include <cstdlib>
 #include <map>
+#include <cstdio>
 #include <mutex>
 #include "psi.cuh"
 #include "net_apply.cuh"
@@ -35,6 +36,8 @@ struct Options {
   double psi_inner_rtol = 1e-6;   // tightest relative tolerance of one FP32 sweep
   int graph = 1;             // vsav_run replays each time step as a CUDA graph
   int psi3d_var = 0;         // 3D: variable psi mobility + BiCGSTAB (the 2D scheme) instead of the constant-M0 division
+  int psi_stop = 0;          // 0: Krylov.jl's stop on ||M^-1 r|| (the reference); 1: on the true residual ||b - A x||
+  int psi_check = 0;         // 1: measure ||b - A x|| / ||b|| of every psi system after each solve
 };
 
 struct StepStatus {
@@ -87,6 +90,8 @@ class SolverBase {
   // snapshots of the psi BiCGSTAB iterates (training data of the network)
   virtual void harvest(int cap) = 0;
   virtual long long harvest_read(float* out, long long cap, int* nsnap) = 0;
+  // the FFT kernel variants this handle uses (JSON text)
+  virtual std::string tuning() = 0;
 };
 
 struct Dims {
@@ -402,6 +407,7 @@ class Solver : public SolverBase {
   float* hv = nullptr;                       // harvested iterates
   int hv_cap = 0, hv_count = 0;
   BiState* bst = nullptr; int *bupd = nullptr, *d_any = nullptr;
+  double* d_true_res = nullptr;     // [3R] measured ||b - A x|| / ||b|| of the last psi solves (psi_check)
   int* h_pinned_any = nullptr;
   StepStatus last;
   double* stage = nullptr;   // host-format staging
@@ -430,6 +436,7 @@ class Solver : public SolverBase {
       : ph(p), opt(o), dm(d) {
     VSAV_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     if (const char* env = getenv("VSAV_PSI_FUSED")) fused_ops = atoi(env) != 0;
+    if (const char* env = getenv("VSAV_PSI_CHUNK_MB")) psi_chunk_mb = atoll(env);
     // VSAV_GRAPH=0 runs every step eagerly (kernel-level profilers see each launch)
     if (const char* env = getenv("VSAV_GRAPH")) if (atoi(env) == 0) opt.graph = 0;
     g.nd = d.nd; g.Nx = d.Nx; g.Ny = d.Ny; g.Nz = (d.nd == 3) ? d.Nz : 1;
@@ -505,6 +512,8 @@ class Solver : public SolverBase {
       vt12 = dalloc<C>((nd == 3 ? 9 : 6) * V * n);
       vx = psi_full() ? dalloc<C>(3 * V * n) : nullptr;
       bst = dalloc<BiState>(3 * R); bupd = dalloc<int>(3 * R); d_any = dalloc<int>(1);
+      d_true_res = dalloc<double>(3 * R);
+      VSAV_CUDA(cudaMemsetAsync(d_true_res, 0, 3 * R * sizeof(double), st));
       VSAV_CUDA(cudaMallocHost(&h_pinned_any, sizeof(int)));
       if (opt.psi_precond < 0 || opt.psi_precond > 2) throw std::runtime_error("psi_precond must be 0, 1 or 2");
       if (opt.psi_precond >= 1 && !opt.psi_mixed) {
@@ -524,10 +533,15 @@ class Solver : public SolverBase {
     stage = dalloc<double>(nh);
     VSAV_CUDA(cudaStreamSynchronize(st));
     autotune();
+    // VSAV_PSI_SPLIT=0/1 overrides the autotuner's choice between the fused and the split
+    // forward pass + combine; read once here, so it holds for this handle's whole life
+    // (graph replays included) and is what the tuning record reports
+    if (const char* env = getenv("VSAV_PSI_SPLIT")) split_comb = atoi(env) != 0;
     if constexpr (std::is_same<T, double>::value) {
       if (opt.psi_mixed && (nd == 2 || opt.psi3d_var)) {
         Options o2 = opt;
         o2.psi_mixed = 0;
+        o2.psi_check = 0;            // the parent measures the FP64 residual after the sweeps
         std::vector<int> rs(dm.R);
         std::vector<double> pin(dm.V), pout(dm.V);
         VSAV_CUDA(cudaMemcpy(pin.data(), d_psi_in, dm.V * sizeof(double), cudaMemcpyDeviceToHost));
@@ -821,13 +835,66 @@ class Solver : public SolverBase {
                 ? Lc : Lr;
     return vE(v) <= L && vE(v) * VNT[v] / L >= 1;
   }
+  // Where this handle's variants came from: "forced" (VSAV_TUNE), "measured", "process" (the
+  // in-memory cache of an earlier handle of the same shape) or "file" (VSAV_TUNE_FILE)
+  const char* tune_source = "measured";
+  // VSAV_TUNE_FILE: a JSON object {key: [variant per family..., split]} that persists the
+  // choices across processes.  A key found there is used as is; a key measured here is
+  // added to the file (rewritten whole, under the process-wide tuning lock).
+  static bool tune_file_read(const char* path, std::map<std::string, std::vector<int>>& out) {
+    FILE* f = fopen(path, "r");
+    if (!f) return false;
+    std::string txt;
+    char buf[4096];
+    size_t n;
+    while ((n = fread(buf, 1, sizeof buf, f)) > 0) txt.append(buf, n);
+    fclose(f);
+    size_t i = 0;
+    while ((i = txt.find('"', i)) != std::string::npos) {
+      size_t j = txt.find('"', i + 1);
+      if (j == std::string::npos) break;
+      std::string key = txt.substr(i + 1, j - i - 1);
+      size_t a = txt.find('[', j), b = txt.find(']', j);
+      if (a == std::string::npos || b == std::string::npos || b < a) break;
+      std::vector<int> v;
+      const char* q = txt.c_str() + a + 1;
+      const char* end = txt.c_str() + b;
+      while (q < end) {
+        char* nx = nullptr;
+        long x = strtol(q, &nx, 10);
+        if (nx == q) { ++q; continue; }
+        v.push_back((int)x);
+        q = nx;
+      }
+      if ((int)v.size() == FAM_N + 1) out[key] = v;
+      i = b + 1;
+    }
+    return true;
+  }
+  static void tune_file_write(const char* path, const std::map<std::string, std::vector<int>>& m) {
+    std::string tmp = std::string(path) + ".tmp";
+    FILE* f = fopen(tmp.c_str(), "w");
+    if (!f) return;
+    fprintf(f, "{\n");
+    size_t k = 0;
+    for (const auto& kv : m) {
+      fprintf(f, "  \"%s\": [", kv.first.c_str());
+      for (size_t i = 0; i < kv.second.size(); ++i) fprintf(f, "%s%d", i ? ", " : "", kv.second[i]);
+      fprintf(f, "]%s\n", ++k < m.size() ? "," : "");
+    }
+    fprintf(f, "}\n");
+    fclose(f);
+    rename(tmp.c_str(), path);
+  }
   void autotune() {
     if (const char* forced = getenv("VSAV_TUNE")) {      // one digit per family: the variant index
       int k = 0;
       for (const char* q = forced; *q && k < FAM_N; ++q)
         if (*q >= '0' && *q <= '9') { int v = *q - '0'; if (v < NVAR && variant_ok(k, v)) choice[k] = v; ++k; }
+      tune_source = "forced";
       return;
     }
+    const char* tfile = getenv("VSAV_TUNE_FILE");
     {
       std::lock_guard<std::mutex> lk(tune_mutex());
       auto it = tune_cache().find(tune_key());
@@ -835,7 +902,25 @@ class Solver : public SolverBase {
         for (int f = 0; f < FAM_N; ++f) choice[f] = it->second[f];
         split_comb = it->second[FAM_N];
         tuned_from_cache = true;
+        tune_source = "process";
         return;
+      }
+      if (tfile && *tfile) {
+        std::map<std::string, std::vector<int>> fm;
+        tune_file_read(tfile, fm);
+        auto jt = fm.find(tune_key());
+        bool ok = jt != fm.end();
+        if (ok)
+          for (int f = 0; f < FAM_N; ++f)
+            if (jt->second[f] < 0 || jt->second[f] >= NVAR || !variant_ok(f, jt->second[f])) ok = false;
+        if (ok) {
+          for (int f = 0; f < FAM_N; ++f) choice[f] = jt->second[f];
+          split_comb = jt->second[FAM_N] != 0;
+          tune_cache()[tune_key()] = jt->second;
+          tuned_from_cache = true;
+          tune_source = "file";
+          return;
+        }
       }
     }
     autotune_measure();
@@ -843,7 +928,27 @@ class Solver : public SolverBase {
     std::vector<int> c(choice, choice + FAM_N);
     c.push_back(split_comb);
     tune_cache()[tune_key()] = c;
+    if (tfile && *tfile) {
+      std::map<std::string, std::vector<int>> fm;
+      tune_file_read(tfile, fm);
+      fm[tune_key()] = c;
+      tune_file_write(tfile, fm);
+    }
   }
+  // the variants in use, as JSON: {"key", "source", "split", families: "E<e>/NT<nt>"}
+  std::string tuning_json() const {
+    static const char* nm[FAM_N] = {"rows_r2c", "rows_c2r", "rows_c2c", "rows_mul", "cols", "cols_psi", "psi_inv2",
+                                    "psi_comb", "psi_fwd2"};
+    std::string o = "{\"key\": \"" + tune_key() + "\", \"source\": \"" + tune_source + "\", \"psi_forward_combine\": \"" +
+                    (split_comb ? "split" : "fused") + "\", \"variants\": {";
+    for (int f = 0; f < FAM_N; ++f)
+      o += std::string(f ? ", " : "") + "\"" + nm[f] + "\": \"E" + std::to_string(vE(choice[f])) + "/NT" +
+           std::to_string(VNT[choice[f]]) + "\"";
+    o += "}";
+    if (psi32) o += ", \"psi_fp32\": " + psi32->tuning_json();
+    return o + "}";
+  }
+  std::string tuning() override { return tuning_json(); }
   static std::mutex& tune_mutex() { static std::mutex m; return m; }
   void autotune_measure() {
     cudaEvent_t e0, e1;
@@ -1347,11 +1452,11 @@ class Solver : public SolverBase {
   // ------------------------------------------------------------------ psi BiCGSTAB (2D)
   // fields per chunk of the psi operator: the chunk's two intermediates stay in L2
   // (chunking is off by default: VSAV_PSI_CHUNK_MB sets the L2 budget of a chunk)
+  long long psi_chunk_mb = 0;  // VSAV_PSI_CHUNK_MB, read when the handle is created (0: no chunking)
   int psi_chunk() const {
-    const char* env = getenv("VSAV_PSI_CHUNK_MB");
-    if (!env) return 3 * dm.V;
+    if (psi_chunk_mb <= 0) return 3 * dm.V;
     const long long per = 2LL * psi_n() * (long long)sizeof(C);
-    long long fc = std::max<long long>(1, (atoll(env) << 20) / per);
+    long long fc = std::max<long long>(1, (psi_chunk_mb << 20) / per);
     return (int)std::min<long long>(fc, 3LL * dm.V);
   }
 
@@ -1359,11 +1464,7 @@ class Solver : public SolverBase {
   // x pass (inverse, x M_psi, forward), y-forward, combine
   EW dot_ew{};                 // partial layout of the dots of the last matvec
   double split_ms = 0.0;
-  // VSAV_PSI_SPLIT=0/1 overrides the autotuner's choice between the fused and the split forward pass
-  bool use_split() const {
-    if (const char* env = getenv("VSAV_PSI_SPLIT")) return atoi(env) != 0;
-    return split_comb != 0;
-  }
+  bool use_split() const { return split_comb != 0; }
   bool fused_ops = true;       // FULL form: fused column passes (VSAV_PSI_FUSED=0: separate kernels)
   void matvec(const C* in, C* out, int mode, const C* svec, bool precond = true) {
     if (g.nd == 3) { matvec3(in, out, mode, svec, precond); return; }
@@ -1462,7 +1563,24 @@ class Solver : public SolverBase {
     if (opt.psi_mixed) { psi_solve_mixed(); return; }
     psi_prepare_b();
     psi_krylov(psi_x(), opt.psi_rtol, opt.psi_itmax);
+    if (opt.psi_check) psi_check_residual(psi_x());
     psi_finish();
+  }
+
+  // psi_check: ||b - A x|| / ||b|| per system of the solve just finished, in this
+  // handle's arithmetic (FP64 for FP64 and mixed handles), into d_true_res
+  void psi_check_residual(const C* x) {
+    const int V = dm.V, R = dm.R, S = 3 * R;
+    const long long F = 3LL * V, n = psi_n();
+    EW e = ew(n);
+    SysMap sm{V, R, d_run_of};
+    VSAV_CUDA(cudaMemsetAsync(bupd, 0xff, S * sizeof(int), st));     // every system active in A x
+    matvec(x, vt, 0, nullptr, false);
+    k_psi_resnorm<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(vb, vt, vgeom(), e, part); VSAV_COUNT_LAUNCH();
+    VSAV_LAUNCH_CHECK();
+    fin(4, (int)F, e, fd);
+    k_psi_true_res<<<(S + 63) / 64, 64, 0, st>>>(fd, d_true_res, sm, S, (int)F); VSAV_COUNT_LAUNCH();
+    VSAV_LAUNCH_CHECK();
   }
 
   // ---- mixed precision: FP32 BiCGSTAB on FP64 residuals (iterative refinement)
@@ -1550,7 +1668,7 @@ class Solver : public SolverBase {
     k_psi_init<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(vb, x, vr, vp, d_adt, mmax_r, ph.S4, vg, sm, e, part); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     fin(4, (int)F, e, fd);
-    k_bi_init<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, bupd, sm, S, (int)F, opt.psi_atol, rtol, itmax); VSAV_COUNT_LAUNCH();
+    k_bi_init<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, bupd, sm, S, (int)F, opt.psi_atol, rtol, itmax, opt.psi_stop); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     if (hv_cap) { hv_count = 0; harvest_snap(x, vr); }
     krylov_loop(itmax, [&]() {
@@ -1562,11 +1680,12 @@ class Solver : public SolverBase {
       matvec(vs, vt, 1, vs);                            // t = M^-1 A s ; <t,s>, <t,t>
       fin(4, (int)F, dot_ew, fd);
       k_bi_omega<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, sm, S, (int)F); VSAV_COUNT_LAUNCH();
-      k_psi_update<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(x, vr, vp, vs, vt, vb, bst, vg, sm, e, part); VSAV_COUNT_LAUNCH();
+      k_psi_update<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(x, vr, vp, vs, vt, vb, bst, vg, sm, e, part, nullptr, d_adt,
+                                                                mmax_r, ph.S4); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
       fin(4, (int)F, e, fd);
       VSAV_CUDA(cudaMemsetAsync(d_any, 0, sizeof(int), st));
-      k_bi_beta<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, bupd, sm, S, (int)F, itmax, d_any); VSAV_COUNT_LAUNCH();
+      k_bi_beta<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, bupd, sm, S, (int)F, itmax, d_any, opt.psi_stop); VSAV_COUNT_LAUNCH();
       k_psi_p<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(vp, vr, vv, bst, bupd, sm, e); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
       if (hv_cap && hv_count < hv_cap) harvest_snap(x, vr);
@@ -1600,7 +1719,7 @@ class Solver : public SolverBase {
     k_psi_init<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(vb, x, vr, vp, d_adt, nullptr, ph.S4, vg, sm, e, part); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     fin(4, (int)F, e, fd);
-    k_bi_init<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, bupd, sm, S, (int)F, opt.psi_atol, rtol, itmax); VSAV_COUNT_LAUNCH();
+    k_bi_init<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, bupd, sm, S, (int)F, opt.psi_atol, rtol, itmax, opt.psi_stop); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
     krylov_loop(itmax, [&]() {
       precond_apply(vp, vph);
@@ -1613,11 +1732,12 @@ class Solver : public SolverBase {
       matvec(vsh, vt, 1, vs, false);                    // t = A s^ ; <t, s>, <t, t>
       fin(4, (int)F, dot_ew, fd);
       k_bi_omega<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, sm, S, (int)F); VSAV_COUNT_LAUNCH();
-      k_psi_update<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(x, vr, vph, vs, vt, vb, bst, vg, sm, e, part, vsh); VSAV_COUNT_LAUNCH();
+      k_psi_update<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(x, vr, vph, vs, vt, vb, bst, vg, sm, e, part, vsh, d_adt,
+                                                                nullptr, ph.S4); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
       fin(4, (int)F, e, fd);
       VSAV_CUDA(cudaMemsetAsync(d_any, 0, sizeof(int), st));
-      k_bi_beta<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, bupd, sm, S, (int)F, itmax, d_any); VSAV_COUNT_LAUNCH();
+      k_bi_beta<<<(S + 63) / 64, 64, 0, st>>>(fd, bst, bupd, sm, S, (int)F, itmax, d_any, opt.psi_stop); VSAV_COUNT_LAUNCH();
       k_psi_p<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(vp, vr, vv, bst, bupd, sm, e); VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
     });
@@ -1835,6 +1955,12 @@ class Solver : public SolverBase {
       }
       return;
     }
+    if (what == 6) {
+      if (!d_true_res) throw std::runtime_error("this handle has no psi BiCGSTAB (3D with constant mobility)");
+      VSAV_CUDA(cudaMemcpyAsync(out, d_true_res, 3 * R * sizeof(double), cudaMemcpyDeviceToHost, st));
+      VSAV_CUDA(cudaStreamSynchronize(st));
+      return;
+    }
     const double* src = what == 0 ? r2 : (what == 1 ? qv : (what == 2 ? theta : (what == 3 ? area : mmax_r)));
     size_t n = what == 0 ? 6 * R : (what == 2 ? 2 * R : (what == 3 ? V : R));
     VSAV_CUDA(cudaMemcpyAsync(out, src, n * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -1950,6 +2076,7 @@ void Solver<T>::psi_solve_mixed() {
       VSAV_LAUNCH_CHECK();
     }
     VSAV_CUDA(cudaMemcpyAsync(bst, H->bst, 3 * R * sizeof(BiState), cudaMemcpyDeviceToDevice, st));
+    if (opt.psi_check) psi_check_residual(x);
     psi_finish();
   }
 }

@@ -78,6 +78,8 @@ void vsav_default_options(vsav_options* o, const vsav_config* cfg) {
   o->device = 0;
   o->graph = 1;
   o->psi3d_variable = 0;
+  o->psi_stop = 0;
+  o->psi_check = 0;
 }
 
 int vsav_create(const vsav_config* cfg, const vsav_options* opt, vsav_handle** out) {
@@ -124,6 +126,9 @@ int vsav_create(const vsav_config* cfg, const vsav_options* opt, vsav_handle** o
     if (o.precision != VSAV_FP64 && o.precision != VSAV_FP32 && o.precision != VSAV_MIXED)
       throw std::runtime_error("precision must be VSAV_FP64, VSAV_FP32 or VSAV_MIXED");
     so.graph = o.graph ? 1 : 0;
+    if (o.psi_stop != 0 && o.psi_stop != 1) throw std::runtime_error("psi_stop must be 0 or 1");
+    so.psi_stop = o.psi_stop;
+    so.psi_check = o.psi_check ? 1 : 0;
     so.psi3d_var = (cfg->ndim == 3 && o.psi3d_variable) ? 1 : 0;
     // mixed: the psi BiCGSTAB in FP32 inside FP64 refinement wherever there is one (2D, 3D variable
     // mobility); otherwise (3D constant mobility) every field stays FP64
@@ -332,6 +337,18 @@ int vsav_time_run(vsav_handle* h, int32_t n0, int32_t nsteps, const double* dt, 
   });
 }
 int64_t vsav_launch_count(void) { return (int64_t)launch_counter().load(); }
+
+int vsav_get_tuning(vsav_handle* h, char* buf, int64_t cap, int64_t* needed) {
+  return guard(h, [&] {
+    const std::string t = h->s->tuning();
+    if (needed) *needed = (int64_t)t.size() + 1;
+    if (buf) {
+      if (cap < (int64_t)t.size() + 1) throw std::runtime_error("tuning buffer too small");
+      memcpy(buf, t.c_str(), t.size() + 1);
+    }
+    return VSAV_OK;
+  });
+}
 
 int vsav_profile(vsav_handle* h, int32_t enable) {
   return guard(h, [&] { h->s->profile(enable); return VSAV_OK; });

@@ -23,7 +23,7 @@ EXPORTS = ("vsav_create", "vsav_destroy", "vsav_last_error", "vsav_create_error"
            "vsav_get_dt", "vsav_set_A0", "vsav_get_A0", "vsav_init_state", "vsav_init_shapes2d", "vsav_generate_initial_condition", "vsav_step1", "vsav_step2", "vsav_step3",
            "vsav_step4", "vsav_step5", "vsav_step6", "vsav_step7", "vsav_update_state", "vsav_run",
            "vsav_monitor", "vsav_get_work", "vsav_get_scalar_work", "vsav_transform", "vsav_time_run",
-           "vsav_profile", "vsav_profile_read", "vsav_launch_count",
+           "vsav_profile", "vsav_profile_read", "vsav_launch_count", "vsav_get_tuning",
            "vsav_net_create", "vsav_net_destroy", "vsav_net_last_error", "vsav_net_nparams",
            "vsav_net_set_params", "vsav_net_get_params", "vsav_net_forward", "vsav_net_grad", "vsav_net_train",
            "vsav_net_eval", "vsav_set_psi_net", "vsav_psi_harvest", "vsav_psi_harvest_read",
@@ -48,7 +48,8 @@ class VsavOptions(ct.Structure):
     _fields_ = [("precision", ct.c_int32), ("psi_form", ct.c_int32), ("psi_precond", ct.c_int32),
                 ("psi_itmax", ct.c_int32), ("psi_rtol", ct.c_double), ("psi_atol", ct.c_double),
                 ("n_runs", ct.c_int32), ("run_sizes", ct.POINTER(ct.c_int32)), ("device", ct.c_int32),
-                ("graph", ct.c_int32), ("psi3d_variable", ct.c_int32)]
+                ("graph", ct.c_int32), ("psi3d_variable", ct.c_int32), ("psi_stop", ct.c_int32),
+                ("psi_check", ct.c_int32)]
 
 
 class VsavShape2D(ct.Structure):
@@ -113,6 +114,7 @@ def load(path: str = LIB_PATH):
         "vsav_profile": ([H, i32], ct.c_int),
         "vsav_profile_read": ([H, i32, D], ct.c_int),
         "vsav_launch_count": ([], ct.c_int64),
+        "vsav_get_tuning": ([H, ct.c_char_p, ct.c_int64, ct.POINTER(ct.c_int64)], ct.c_int),
         "vsav_irfft2d_f32_noalloc": ([ct.c_void_p, ct.c_void_p, i32, i32, i32, ct.c_double, ct.c_double, i32,
                                       ct.c_void_p], ct.c_int),
         "vsav_noalloc_error": ([], ct.c_char_p),

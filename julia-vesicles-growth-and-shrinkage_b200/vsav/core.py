@@ -35,7 +35,8 @@ class Handle:
     def __init__(self, cfg, precision: str = "fp64", psi_form: Optional[str] = None,
                  run_sizes: Optional[Sequence[int]] = None, psi_itmax: int = 20,
                  psi_rtol: Optional[float] = None, psi_atol: float = 1e-14, device: int = 0,
-                 psi_precond: str = "diag", psi_net=None, graph: bool = True, psi3d_variable: bool = False):
+                 psi_precond: str = "diag", psi_net=None, graph: bool = True, psi3d_variable: bool = False,
+                 psi_stop: str = "krylov", psi_check: bool = False):
         """cfg: any object with the reference Config fields (Types.jl:27-74);
         psi_in_v / psi_out_v hold one value per vesicle field of all runs.
         psi_precond: "diag" (the reference's left-preconditioned BiCGSTAB),
@@ -44,7 +45,10 @@ class Handle:
         psi_net gives: an array of 7409 values or a path to an .npz with
         "theta").  psi3d_variable: 3D Step 1 with the 2D scheme's variable psi
         mobility and BiCGSTAB instead of the reference's constant-mobility
-        spectral division."""
+        spectral division.  psi_stop: "krylov" (Krylov.jl's stop on the
+        preconditioned residual, the reference) or "true" (stop on ||b - A x||).
+        psi_check: measure ||b - A x|| / ||b|| of every psi system after each
+        solve (true_residuals())."""
         self.lib = L.load()
         self.nd = 3 if getattr(cfg, "Nz", 0) else 2
         self.Nx, self.Ny = int(cfg.Nx), int(cfg.Ny)
@@ -75,6 +79,9 @@ class Handle:
         o.psi_precond = PSI_PRECOND[psi_precond]
         o.graph = 1 if graph else 0
         o.psi3d_variable = 1 if psi3d_variable else 0
+        self.psi3d_variable = bool(psi3d_variable)
+        o.psi_stop = {"krylov": 0, "true": 1}[psi_stop]
+        o.psi_check = 1 if psi_check else 0
         self.psi_precond = psi_precond
         o.psi_itmax = psi_itmax
         o.psi_rtol = cfg.tol if psi_rtol is None else psi_rtol
@@ -328,13 +335,31 @@ class Handle:
         return a
 
     def scalar_work(self, what):
-        n = {0: 6 * self.R, 1: self.R, 2: 2 * self.R, 3: self.V, 4: self.R, 5: 12 * self.R}[what]
+        n = {0: 6 * self.R, 1: self.R, 2: 2 * self.R, 3: self.V, 4: self.R, 5: 12 * self.R, 6: 3 * self.R}[what]
         a = np.empty(n)
         self._chk(self.lib.vsav_get_scalar_work(self.h, what, L.dptr(a)))
         return a
 
     def psi_stats(self):
         return self.scalar_work(5).reshape(3 * self.R, 4)
+
+    def has_psi_solve(self):
+        """True where Step 1 solves psi by BiCGSTAB (2D, or 3D with psi3d_variable)."""
+        return self.nd == 2 or self.psi3d_variable
+
+    def true_residuals(self):
+        """||b - A x|| / ||b|| of each psi system of the last Step 1 (needs psi_check)."""
+        return self.scalar_work(6)
+
+    def tuning(self):
+        """The FFT kernel variants this handle uses and where they came from
+        (vsav_get_tuning), as a dict."""
+        import json
+        need = ct.c_int64()
+        self._chk(self.lib.vsav_get_tuning(self.h, None, 0, ct.byref(need)))
+        buf = ct.create_string_buffer(need.value)
+        self._chk(self.lib.vsav_get_tuning(self.h, buf, need.value, ct.byref(need)))
+        return json.loads(buf.value.decode())
 
     # -- transforms ---------------------------------------------------------
     def rfft(self, f):
