@@ -242,6 +242,114 @@ __device__ __forceinline__ int tile_fft(C (&v)[E], C* const (&buf)[2], const Lay
 }
 
 
+// ---------------------------------------------------------------------------
+// Single-buffer variants (half the shared memory of the ping-pong passes): a
+// pass reads all of its butterflies into registers, waits for every thread,
+// then writes.  Every thread holds E / R butterflies of every pass, so the
+// block must cover the whole tile (blockDim.x * E = lines * L).  The butterflies, their twiddles and the radix split are those
+// of stockham_pass / smem_passes / tile_fft, so the results are bit-identical.
+// ---------------------------------------------------------------------------
+template <int R, int E, bool INV, typename C, typename Lay>
+__device__ __forceinline__ void stockham_pass_1buf(C* buf, const Lay lay, int logL, int lognl, int p,
+                                                   const C* __restrict__ tab) {
+  constexpr int NB = E / R;
+  constexpr int LGR = Log2<R>::v;
+  const int logLR = logL - LGR;
+  const int LR = 1 << logLR;
+  const int nthr = blockDim.x, tid = threadIdx.x;
+  C v[NB][R];
+#pragma unroll
+  for (int q = 0; q < NB; ++q) {
+    const int b = q * nthr + tid;
+    int line, i;
+    if (Lay::line_fast) { line = b & ((1 << lognl) - 1); i = b >> lognl; }
+    else { line = b >> logLR; i = b & (LR - 1); }
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[q][r] = buf[lay(line, i + r * LR)];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < NB; ++q) {
+    const int b = q * nthr + tid;
+    int line, i;
+    if (Lay::line_fast) { line = b & ((1 << lognl) - 1); i = b >> lognl; }
+    else { line = b >> logLR; i = b & (LR - 1); }
+    const int k = i & (p - 1);
+    if (p > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        C w = __ldg(&tab[p * R + r * k]);
+        if (INV) w.y = -w.y;
+        v[q][r] = v[q][r] * w;
+      }
+    }
+    dft_reg<R, INV>(v[q]);
+    const int o = (i - k) * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) buf[lay(line, o + r * p)] = v[q][r];
+  }
+  __syncthreads();
+}
+
+template <int E, bool INV, typename C, typename Lay>
+__device__ __forceinline__ void smem_passes_1buf(C* buf, const Lay lay, int logL, int lognl, int p, int bits,
+                                                 const C* __restrict__ tab) {
+  constexpr int LOGE = Log2<E>::v < 5 ? Log2<E>::v : 5;
+  if (bits <= 0) return;
+  const int npass = (bits + LOGE - 1) / LOGE;
+  const int base = bits / npass, extra = bits % npass;
+  for (int ip = 0; ip < npass; ++ip) {
+    const int lr = base + (ip < extra ? 1 : 0);
+    switch (lr) {
+      case 1: stockham_pass_1buf<2, E, INV>(buf, lay, logL, lognl, p, tab); break;
+      case 2: if constexpr (E >= 4) stockham_pass_1buf<4, E, INV>(buf, lay, logL, lognl, p, tab); break;
+      case 3: if constexpr (E >= 8) stockham_pass_1buf<8, E, INV>(buf, lay, logL, lognl, p, tab); break;
+      case 4: if constexpr (E >= 16) stockham_pass_1buf<16, E, INV>(buf, lay, logL, lognl, p, tab); break;
+      default:
+        if constexpr (E >= 32) stockham_pass_1buf<32, E, INV>(buf, lay, logL, lognl, p, tab);
+        break;
+    }
+    p <<= lr;
+  }
+}
+
+// tile_fft with the input in v[] and the output returned in v[] (ENTRY_REG and
+// EXIT_REG), through one shared-memory buffer.  Needs L >= E^2 and every
+// thread of the block holding one butterfly (a full tile).
+template <int E, bool INV, typename C, typename Lay>
+__device__ __forceinline__ void tile_fft_1buf(C (&v)[E], C* buf, const Lay lay, int line, int i, int logL, int lognl,
+                                              const C* __restrict__ tab) {
+  constexpr int LOGE = Log2<E>::v;
+  const int LE = 1 << (logL - LOGE);
+  dft_reg<E, INV>(v);
+#pragma unroll
+  for (int r = 0; r < E; ++r) buf[lay(line, i * E + r)] = v[r];
+  __syncthreads();
+  smem_passes_1buf<E, INV>(buf, lay, logL, lognl, E, logL - 2 * LOGE, tab);
+#pragma unroll
+  for (int r = 0; r < E; ++r) v[r] = buf[lay(line, i + r * LE)];
+  if constexpr (E >= 16) {
+    C lo[4], hi[E / 4];
+#pragma unroll
+    for (int q = 1; q < 4; ++q) { lo[q] = __ldg(&tab[(1 << logL) + q * i]); if (INV) lo[q].y = -lo[q].y; }
+#pragma unroll
+    for (int q = 1; q < E / 4; ++q) { hi[q] = __ldg(&tab[(1 << logL) + 4 * q * i]); if (INV) hi[q].y = -hi[q].y; }
+#pragma unroll
+    for (int r = 1; r < E; ++r) {
+      C w = (r & 3) == 0 ? hi[r >> 2] : ((r >> 2) == 0 ? lo[r & 3] : hi[r >> 2] * lo[r & 3]);
+      v[r] = v[r] * w;
+    }
+  } else {
+#pragma unroll
+    for (int r = 1; r < E; ++r) {
+      C w = __ldg(&tab[(1 << logL) + r * i]);
+      if (INV) w.y = -w.y;
+      v[r] = v[r] * w;
+    }
+  }
+  dft_reg<E, INV>(v);
+}
+
 // minimum resident CTAs that the register budget must allow, per (E, NT)
 template <int E, int NT> struct MinB {
   static constexpr int v = (NT >= 1024) ? 1 : (NT >= 512) ? ((E <= 8) ? 2 : 1) : ((E <= 4) ? 4 : ((E <= 8) ? 3 : 2));

@@ -23,6 +23,7 @@
 //        by up to ~1e-2, so FULL is the default in both precisions.
 #pragma once
 #include "kernels.cuh"
+#include "tma.cuh"
 
 namespace vsav {
 
@@ -403,6 +404,234 @@ __global__ void __launch_bounds__(NT, MinB<E, NT>::v) k_psi_cols_comb(const cplx
     }
   }
   block_reduce_store<4>(acc, part + ((long long)f * a.tiles + tile) * 4, smm);
+}
+
+// ---------------------------------------------------------------------------
+// TMA-fed persistent forms of the two FULL-form column passes (FP32).
+//
+// A tile is TW consecutive columns of one field, all L rows.  Each block is
+// resident for the whole launch and walks the tiles blockIdx.x, + gridDim.x,
+// ...; the inputs of a tile arrive in a shared-memory staging area by 2D bulk
+// tensor copies (one thread issues them; boxes of TW columns x min(L, 256)
+// rows), so the copies of tile k+1 run while tile k is transformed.  The two
+// transforms of a tile (t1 and t2, or the two derivative directions) run as
+// one tile of 2 TW lines through the single-buffer FFT, whose arithmetic is
+// that of the ping-pong kernels: the transforms are bit-identical to those of
+// k_psi_cols_inv2 / k_psi_cols_comb.
+//
+// Shared memory (dynamic, 1024-byte aligned):
+//   staging  A arrays x [L][TW] (TMA box layout), A = 1 (inv2) or 4 (comb: t1 t2 x c)
+//   work     col_tile_elems(L, 2 TW, log2 E) complex (the FFT buffer)
+//   2 mbarriers
+// ---------------------------------------------------------------------------
+struct TmaTiles {
+  int total;        // tiles over the chunk's fields: fc * tiles
+  int tiles;        // column tiles per field: Nx / TW
+  int TW, logTW;
+  int BH, nbox;     // rows per box, boxes per column tile (BH * nbox = L)
+};
+
+__host__ __device__ __forceinline__ size_t tma_col_smem(int L, int TW, int E, int narrays) {
+  const size_t stage = (size_t)narrays * L * TW * sizeof(float2);
+  int loge = 0;
+  while ((1 << loge) < E) ++loge;
+  const size_t work = (size_t)col_tile_elems(L, 2 * TW, loge) * sizeof(float2);
+  return 1024 + stage + work + 64;
+}
+
+__device__ __forceinline__ unsigned char* tma_smem_base() {
+  extern __shared__ __align__(16) unsigned char smraw_tma[];
+  return reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smraw_tma) + 1023) & ~(uintptr_t)1023);
+}
+
+// Inverse y pass of both derivative directions (k_psi_cols_inv2, FP32):
+//   t1 = IFFT_y(i kx0 S4 x),  t2 = IFFT_y(i ky S4 x)   (x global field f0 + fl; t1/t2 chunk-local fl)
+template <int E, int NT>
+__global__ void __launch_bounds__(NT, NT <= 512 ? 2 : 1) k_psi_cols_inv2_tma(const __grid_constant__ CUtensorMap mx, float2* __restrict__ t1,
+                                                              float2* __restrict__ t2, double S4, ColArgs a, TmaTiles tt,
+                                                              SysMap sm, const int* __restrict__ active, int f0,
+                                                              const float2* __restrict__ tab, int* __restrict__ err) {
+  using C = float2;
+  unsigned char* base = tma_smem_base();
+  const int L = 1 << a.logL, LE = L / E, TW = tt.TW;
+  C* sx = reinterpret_cast<C*>(base);
+  C* work = sx + (size_t)L * TW;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(work + col_tile_elems(L, 2 * TW, Log2<E>::v));
+  const int tid = threadIdx.x, lognl = tt.logTW + 1;
+  const int line = tid & (2 * TW - 1), i = tid >> lognl, cl = line & (TW - 1);
+  const bool dir_y = line >= TW;
+  const uint32_t tx = (uint32_t)((size_t)L * TW * sizeof(C));
+  auto act = [&](int t) { return !active || active[sm.sys(f0 + t / tt.tiles)]; };
+  auto next = [&](int t) { while (t < tt.total && !act(t)) t += gridDim.x; return t; };
+  auto issue = [&](int t) {
+    const int fl = t / tt.tiles, c0 = (t % tt.tiles) * TW;
+    mbar_arrive_expect_tx(bar, tx);
+    for (int q = 0; q < tt.nbox; ++q) tma_load_2d(sx + (size_t)q * tt.BH * TW, &mx, c0, (f0 + fl) * a.Ny + q * tt.BH, bar);
+  };
+  if (tid == 0) { mbar_init(bar, 1); mbar_fence_init(); }
+  __syncthreads();
+  int t = next(blockIdx.x);
+  if (tid == 0 && t < tt.total) issue(t);
+  const ColLay lay{2 * TW, Log2<E>::v};
+  const float fi = (float)i, fLE = (float)LE, fNy = (float)a.Ny, fky = (float)(a.kys * S4);
+  uint32_t ph = 0;
+  while (t < tt.total) {
+    const int fl = t / tt.tiles, c = (t % tt.tiles) * TW + cl;
+    const bool ok = mbar_wait(bar, ph, err);
+    if (__syncthreads_or(!ok)) return;
+    const float fkx = (float)(kfreq(c, a.Nx) * a.kxs * S4);
+    C v[E];
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const C xv = sx[(i + j * LE) * TW + cl];
+      float k = fkx;
+      if (dir_y) {
+        float ke = fmaf((float)j, fLE, fi);
+        if (i + j * LE >= (a.Ny >> 1)) ke -= fNy;
+        k = ke * fky;
+      }
+      v[j] = mk<C>(-k * xv.y, k * xv.x);
+    }
+    __syncthreads();                                          // staging consumed by every thread
+    const int tn = next(t + gridDim.x);
+    if (tid == 0 && tn < tt.total) { fence_proxy_async(); issue(tn); }
+    tile_fft_1buf<E, true>(v, work, lay, line, i, a.logL, lognl, tab);
+    C* o = (dir_y ? t2 : t1) + (long long)fl * a.O + c;
+#pragma unroll
+    for (int j = 0; j < E; ++j) o[(long long)(i + j * LE) * a.S] = v[j];
+    __syncthreads();                                          // work buffer free for the next tile
+    ph ^= 1;
+    t = tn;
+  }
+}
+
+// Forward y pass of t1 and t2 fused with the operator output, the diagonal
+// preconditioner and the dot products (k_psi_cols_comb, FP32, x given):
+//   y = P^-1 (a_dt x - (i kx0 t1^ + i ky t2^)); mode 0: dots <c, y>; mode 1: <y, s>, <y, y>.
+// The two transforms are lines 0..TW-1 (t1) and TW..2TW-1 (t2) of one tile; the
+// holders of a column's t1 and t2 sit TW lanes apart and trade halves of their
+// elements by shuffle, so each computes the epilogue of E/2 rows.  Unlike
+// k_psi_cols_comb, whose epilogue runs in FP64, y is formed in FP32 (its
+// transforms are bit-identical; y differs by FP32 rounding), with the dots in FP64.
+template <int E, int NT>
+__global__ void __launch_bounds__(NT, 1) k_psi_cols_comb_tma(
+    const __grid_constant__ CUtensorMap mt1, const __grid_constant__ CUtensorMap mt2,
+    const __grid_constant__ CUtensorMap mx, const __grid_constant__ CUtensorMap mc, float2* __restrict__ y, int mode,
+    const double* __restrict__ adt_r, const double* __restrict__ mmax_r, double S4, ColArgs a, TmaTiles tt, SysMap sm,
+    const int* __restrict__ active, int f0, const float2* __restrict__ tab, double2* __restrict__ part,
+    int* __restrict__ err) {
+  using C = float2;
+  __shared__ double smm[2 * 4 * (NT / 32)];
+  unsigned char* base = tma_smem_base();
+  const int L = 1 << a.logL, LE = L / E, TW = tt.TW;
+  const size_t tile_n = (size_t)L * TW;
+  C* s1 = reinterpret_cast<C*>(base);
+  C* s2 = s1 + tile_n;
+  C* sxv = s2 + tile_n;
+  C* scv = sxv + tile_n;
+  C* work = scv + tile_n;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(work + col_tile_elems(L, 2 * TW, Log2<E>::v));   // [0] t1 t2, [1] x c
+  const int tid = threadIdx.x, lognl = tt.logTW + 1;
+  const int line = tid & (2 * TW - 1), i = tid >> lognl, cl = line & (TW - 1);
+  const bool is1 = line < TW;
+  const uint32_t tx2 = (uint32_t)(2 * tile_n * sizeof(C));
+  auto act = [&](int t) { return !active || active[sm.sys(f0 + t / tt.tiles)]; };
+  auto next = [&](int t) { while (t < tt.total && !act(t)) t += gridDim.x; return t; };
+  auto issue_t = [&](int t) {
+    const int fl = t / tt.tiles, c0 = (t % tt.tiles) * TW;
+    mbar_arrive_expect_tx(&bar[0], tx2);
+    for (int q = 0; q < tt.nbox; ++q) {
+      tma_load_2d(s1 + (size_t)q * tt.BH * TW, &mt1, c0, fl * a.Ny + q * tt.BH, &bar[0]);
+      tma_load_2d(s2 + (size_t)q * tt.BH * TW, &mt2, c0, fl * a.Ny + q * tt.BH, &bar[0]);
+    }
+  };
+  auto issue_xc = [&](int t) {
+    const int fl = t / tt.tiles, c0 = (t % tt.tiles) * TW;
+    mbar_arrive_expect_tx(&bar[1], tx2);
+    for (int q = 0; q < tt.nbox; ++q) {
+      tma_load_2d(sxv + (size_t)q * tt.BH * TW, &mx, c0, (f0 + fl) * a.Ny + q * tt.BH, &bar[1]);
+      tma_load_2d(scv + (size_t)q * tt.BH * TW, &mc, c0, (f0 + fl) * a.Ny + q * tt.BH, &bar[1]);
+    }
+  };
+  if (tid == 0) { mbar_init(&bar[0], 1); mbar_init(&bar[1], 1); mbar_fence_init(); }
+  __syncthreads();
+  // tiles of inactive systems get zero dot partials (the per-tile layout of k_psi_cols_comb)
+  for (int t = blockIdx.x; t < tt.total; t += gridDim.x)
+    if (!act(t) && tid < 4) part[((long long)(f0 + t / tt.tiles) * tt.tiles + t % tt.tiles) * 4 + tid] = make_double2(0.0, 0.0);
+  int t = next(blockIdx.x);
+  if (tid == 0 && t < tt.total) { issue_t(t); issue_xc(t); }
+  const ColLay lay{2 * TW, Log2<E>::v};
+  uint32_t ph = 0;
+  while (t < tt.total) {
+    const int fl = t / tt.tiles, tile = t % tt.tiles, f = f0 + fl, c = tile * TW + cl;
+    bool ok = mbar_wait(&bar[0], ph, err);
+    if (__syncthreads_or(!ok)) return;
+    C v[E];
+    const C* st = is1 ? s1 : s2;
+#pragma unroll
+    for (int j = 0; j < E; ++j) v[j] = st[(i + j * LE) * TW + cl];
+    __syncthreads();                                          // t1 / t2 staging consumed
+    const int tn = next(t + gridDim.x);
+    if (tid == 0 && tn < tt.total) { fence_proxy_async(); issue_t(tn); }
+    tile_fft_1buf<E, false>(v, work, lay, line, i, a.logL, lognl, tab);
+    // trade halves with the partner TW lanes away: the t1 holder keeps rows j < E/2,
+    // the t2 holder rows j >= E/2
+    constexpr int H = E / 2;
+    C w1[H], w2[H];
+#pragma unroll
+    for (int h = 0; h < H; ++h) {
+      const C snd = is1 ? v[h + H] : v[h];
+      C rcv;
+      rcv.x = __shfl_xor_sync(0xffffffffu, snd.x, TW);
+      rcv.y = __shfl_xor_sync(0xffffffffu, snd.y, TW);
+      w1[h] = is1 ? v[h] : rcv;                               // t1^ at the row this thread finishes
+      w2[h] = is1 ? rcv : v[h + H];                           // t2^
+    }
+    ok = mbar_wait(&bar[1], ph, err);
+    if (__syncthreads_or(!ok)) return;
+    // epilogue in FP32 (the solver's arithmetic), the dot products of the stored FP32
+    // values in FP64: a plain FP64 sum over this thread's E/2 rows, compensated across
+    // threads and blocks
+    double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+    {
+      const int r = sm.run_of[f % sm.V];
+      const float adt = (float)adt_r[r], mms4 = mmax_r ? (float)(mmax_r[r] * S4) : 0.f;
+      const float kx = (float)(kfreq(c, a.Nx) * a.kxs), fky = (float)a.kys;
+      const float fi = (float)i, fLE = (float)LE, fNy = (float)a.Ny;
+      C* yo = y + (long long)f * a.O + c;
+#pragma unroll
+      for (int h = 0; h < H; ++h) {
+        const int jj = is1 ? h : h + H;
+        const int e = i + jj * LE;
+        float ke = fmaf((float)jj, fLE, fi);
+        if (e >= (a.Ny >> 1)) ke -= fNy;
+        const float ky = ke * fky;
+        const C xv = sxv[e * TW + cl], cv = scv[e * TW + cl];
+        float ox = fmaf(adt, xv.x, fmaf(kx, w1[h].y, ky * w2[h].y));
+        float oy = fmaf(adt, xv.y, -fmaf(kx, w1[h].x, ky * w2[h].x));
+        if (mmax_r) {
+          const float pinv = 1.0f / fmaf(mms4, fmaf(kx, kx, ky * ky), adt);
+          ox *= pinv; oy *= pinv;
+        }
+        yo[(long long)e * a.S] = mk<C>(ox, oy);
+        const double dx = ox, dy = oy, cx = cv.x, cy = cv.y;
+        if (mode == 0) {
+          d0 = fma(cx, dx, fma(cy, dy, d0));
+          d1 = fma(cx, dy, fma(-cy, dx, d1));
+        } else {
+          d0 = fma(dx, cx, fma(dy, cy, d0));
+          d1 = fma(dx, cy, fma(-dy, cx, d1));
+          d2 = fma(dx, dx, fma(dy, dy, d2));
+        }
+      }
+    }
+    KSum acc[4] = {{d0, 0}, {d1, 0}, {d2, 0}, {0, 0}};
+    __syncthreads();                                          // x / c staging consumed
+    if (tid == 0 && tn < tt.total) { fence_proxy_async(); issue_xc(tn); }
+    block_reduce_store<4>(acc, part + ((long long)f * tt.tiles + tile) * 4, smm);
+    ph ^= 1;
+    t = tn;
+  }
 }
 
 // The 3D full-spectrum operator output (the 2D FULL form with a z direction):

@@ -537,6 +537,8 @@ class Solver : public SolverBase {
     // forward pass + combine; read once here, so it holds for this handle's whole life
     // (graph replays included) and is what the tuning record reports
     if (const char* env = getenv("VSAV_PSI_SPLIT")) split_comb = atoi(env) != 0;
+    // VSAV_PSI_TMA=0/1 overrides the choice of the TMA-fed psi column passes (where eligible)
+    if (const char* env = getenv("VSAV_PSI_TMA")) tma_cols = atoi(env) != 0 && tma_eligible();
     if constexpr (std::is_same<T, double>::value) {
       if (opt.psi_mixed && (nd == 2 || opt.psi3d_var)) {
         Options o2 = opt;
@@ -821,6 +823,110 @@ class Solver : public SolverBase {
     return tiles;
   }
 
+  // ---- TMA-fed persistent column passes of the FULL psi operator (FP32) ----
+  // One tile: TW = E * NT / (2 L) columns, t1 and t2 (or both directions) as 2 TW lines.
+  // Two block shapes with the same tile (E * NT = 8192): variant 0 E 16 / NT 512,
+  // variant 1 E 8 / NT 1024; the autotuner picks one per pass.
+  static constexpr int TMA_TILE = 8192;
+  static constexpr int TMA_VE[2] = {16, 8}, TMA_VNT[2] = {512, 1024};
+  int tma_cols = 0;               // 1: the psi column passes run as the TMA-fed kernels (autotuned)
+  int tma_var_inv2 = 0, tma_var_comb = 0;
+  int tma_ctas[2][2] = {{0, 0}, {0, 0}};     // [pass][variant] resident blocks (grid of the persistent launch)
+  std::map<std::pair<const void*, long long>, CUtensorMap> tmaps;
+  bool tma_eligible() const {
+    if constexpr (!std::is_same<T, float>::value) return false;
+    else {
+      if (g.nd != 2 || !psi_full() || vt12 == nullptr) return false;
+      const int L = g.Ny;
+      if (L < TMA_VE[0] * TMA_VE[0] || L > 4096) return false;   // the single-buffer FFT needs L >= E^2
+      const int TW = TMA_TILE / (2 * L);
+      return TW >= 2 && TW <= 16 && g.Nx % TW == 0;
+    }
+  }
+  TmaTiles tma_tiles(int fc) const {
+    TmaTiles tt{};
+    const int L = g.Ny;
+    tt.TW = TMA_TILE / (2 * L);
+    tt.logTW = ilog2(tt.TW);
+    tt.tiles = g.Nx / tt.TW;
+    tt.total = fc * tt.tiles;
+    tt.BH = std::min(L, 256);
+    tt.nbox = L / tt.BH;
+    return tt;
+  }
+  const CUtensorMap* tmap(const C* base, long long rows, int TW, int BH) {
+    auto key = std::make_pair((const void*)base, rows * 4096 + TW * 512 + BH);
+    auto it = tmaps.find(key);
+    if (it == tmaps.end()) it = tmaps.emplace(key, make_tile_map(base, (int)sizeof(C), rows, g.Nx, TW, BH)).first;
+    return &it->second;
+  }
+  int tma_grid(const void* fn, int nt, size_t smem, int& cache) {
+    if (!cache) {
+      VSAV_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      int per = 0, dev = 0, nsm = 0;
+      VSAV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, nt, smem));
+      VSAV_CUDA(cudaGetDevice(&dev));
+      VSAV_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+      if (per < 1) throw std::runtime_error("TMA column pass does not fit on an SM");
+      cache = per * nsm;
+    }
+    return cache;
+  }
+  template <int E_, int NT_>
+  void launch_inv2_tma(const C* x, C* t1, C* t2, int f0, int fc, bool use_active, int var) {
+    if constexpr (std::is_same<T, float>::value) {
+      SysMap sm{dm.V, dm.R, d_run_of};
+      long long nouter = fc;
+      ColArgs a = colargs(3, nouter, E_, NT_);
+      TmaTiles tt = tma_tiles(fc);
+      const size_t smem = tma_col_smem(g.Ny, tt.TW, E_, 1);
+      const CUtensorMap* mx = tmap(x, 3LL * dm.V * g.Ny, tt.TW, tt.BH);
+      const int grid = std::min(tt.total, tma_grid((const void*)k_psi_cols_inv2_tma<E_, NT_>, NT_, smem, tma_ctas[0][var]));
+      prof.begin(st);
+      k_psi_cols_inv2_tma<E_, NT_><<<grid, NT_, smem, st>>>(*mx, t1, t2, ph.S4, a, tt, sm, use_active ? bupd : nullptr, f0,
+                                                             tab, d_err);
+      VSAV_COUNT_LAUNCH();
+      VSAV_LAUNCH_CHECK();
+      prof.end(st, KC_COLS_F32, (double)fc * g.Pfull * 3.0 * sizeof(C));
+    }
+  }
+  template <int E_, int NT_>
+  int launch_comb_tma(const C* t1, const C* t2, const C* x, C* y, int mode, const C* svec, const double* pre, int f0,
+                      int fc, bool use_active, int var) {
+    if constexpr (std::is_same<T, float>::value) {
+      SysMap sm{dm.V, dm.R, d_run_of};
+      long long nouter = fc;
+      ColArgs a = colargs(3, nouter, E_, NT_);
+      TmaTiles tt = tma_tiles(fc);
+      const size_t smem = tma_col_smem(g.Ny, tt.TW, E_, 4);
+      const long long rows_g = 3LL * dm.V * g.Ny, rows_c = (long long)fc * g.Ny;
+      const CUtensorMap* m1 = tmap(t1, rows_c, tt.TW, tt.BH);
+      const CUtensorMap* m2 = tmap(t2, rows_c, tt.TW, tt.BH);
+      const CUtensorMap* mx = tmap(x, rows_g, tt.TW, tt.BH);
+      const CUtensorMap* mc = tmap(mode == 0 ? vb : svec, rows_g, tt.TW, tt.BH);
+      const int grid = std::min(tt.total, tma_grid((const void*)k_psi_cols_comb_tma<E_, NT_>, NT_, smem, tma_ctas[1][var]));
+      prof.begin(st);
+      k_psi_cols_comb_tma<E_, NT_><<<grid, NT_, smem, st>>>(*m1, *m2, *mx, *mc, y, mode, d_adt, pre, ph.S4, a, tt, sm,
+                                                             use_active ? bupd : nullptr, f0, tab, part, d_err);
+      VSAV_COUNT_LAUNCH();
+      VSAV_LAUNCH_CHECK();
+      prof.end(st, KC_PSI_VEC, (double)fc * g.Pfull * 5.0 * sizeof(C));
+      return tt.tiles;
+    }
+    return 0;
+  }
+  void psi_cols_inv2_tma(const C* x, C* t1, C* t2, int f0, int fc, bool use_active, int var = -1) {
+    if (var < 0) var = tma_var_inv2;
+    if (var == 0) launch_inv2_tma<TMA_VE[0], TMA_VNT[0]>(x, t1, t2, f0, fc, use_active, 0);
+    else launch_inv2_tma<TMA_VE[1], TMA_VNT[1]>(x, t1, t2, f0, fc, use_active, 1);
+  }
+  int psi_cols_comb_tma(const C* t1, const C* t2, const C* x, C* y, int mode, const C* svec, const double* pre, int f0,
+                        int fc, bool use_active, int var = -1) {
+    if (var < 0) var = tma_var_comb;
+    if (var == 0) return launch_comb_tma<TMA_VE[0], TMA_VNT[0]>(t1, t2, x, y, mode, svec, pre, f0, fc, use_active, 0);
+    return launch_comb_tma<TMA_VE[1], TMA_VNT[1]>(t1, t2, x, y, mode, svec, pre, f0, fc, use_active, 1);
+  }
+
   // time every variant of every pass family on scratch buffers; keep the fastest
   // process-wide tuning cache: handles of the same shape reuse the first choice
   static std::map<std::string, std::vector<int>>& tune_cache() { static std::map<std::string, std::vector<int>> m; return m; }
@@ -866,7 +972,7 @@ class Solver : public SolverBase {
         v.push_back((int)x);
         q = nx;
       }
-      if ((int)v.size() == FAM_N + 1) out[key] = v;
+      if ((int)v.size() == FAM_N + 2) out[key] = v;
       i = b + 1;
     }
     return true;
@@ -901,6 +1007,7 @@ class Solver : public SolverBase {
       if (it != tune_cache().end()) {
         for (int f = 0; f < FAM_N; ++f) choice[f] = it->second[f];
         split_comb = it->second[FAM_N];
+        tma_from_code(it->second[FAM_N + 1]);
         tuned_from_cache = true;
         tune_source = "process";
         return;
@@ -916,6 +1023,7 @@ class Solver : public SolverBase {
         if (ok) {
           for (int f = 0; f < FAM_N; ++f) choice[f] = jt->second[f];
           split_comb = jt->second[FAM_N] != 0;
+          tma_from_code(jt->second[FAM_N + 1]);
           tune_cache()[tune_key()] = jt->second;
           tuned_from_cache = true;
           tune_source = "file";
@@ -927,6 +1035,7 @@ class Solver : public SolverBase {
     std::lock_guard<std::mutex> lk(tune_mutex());
     std::vector<int> c(choice, choice + FAM_N);
     c.push_back(split_comb);
+    c.push_back(tma_cols | tma_var_inv2 << 1 | tma_var_comb << 2);
     tune_cache()[tune_key()] = c;
     if (tfile && *tfile) {
       std::map<std::string, std::vector<int>> fm;
@@ -935,12 +1044,22 @@ class Solver : public SolverBase {
       tune_file_write(tfile, fm);
     }
   }
+  void tma_from_code(int code) {
+    tma_cols = (code & 1) && tma_eligible();
+    tma_var_inv2 = (code >> 1) & 1;
+    tma_var_comb = (code >> 2) & 1;
+  }
   // the variants in use, as JSON: {"key", "source", "split", families: "E<e>/NT<nt>"}
   std::string tuning_json() const {
     static const char* nm[FAM_N] = {"rows_r2c", "rows_c2r", "rows_c2c", "rows_mul", "cols", "cols_psi", "psi_inv2",
                                     "psi_comb", "psi_fwd2"};
     std::string o = "{\"key\": \"" + tune_key() + "\", \"source\": \"" + tune_source + "\", \"psi_forward_combine\": \"" +
-                    (split_comb ? "split" : "fused") + "\", \"variants\": {";
+                    (split_comb ? "split" : "fused") + "\", \"psi_column_passes\": \"" +
+                    (tma_cols ? "tma" : "classic") + "\", \"variants\": {";
+    if (tma_cols)
+      o += "\"psi_inv2_tma\": \"E" + std::to_string(TMA_VE[tma_var_inv2]) + "/NT" + std::to_string(TMA_VNT[tma_var_inv2]) +
+           "\", \"psi_comb_tma\": \"E" + std::to_string(TMA_VE[tma_var_comb]) + "/NT" +
+           std::to_string(TMA_VNT[tma_var_comb]) + "\", ";
     for (int f = 0; f < FAM_N; ++f)
       o += std::string(f ? ", " : "") + "\"" + nm[f] + "\": \"E" + std::to_string(vE(choice[f])) + "/NT" +
            std::to_string(VNT[choice[f]]) + "\"";
@@ -1014,6 +1133,35 @@ class Solver : public SolverBase {
       // the fused form (fewer bytes) unless the split pair is clearly faster
       split_comb = split_ms < 0.95 * tune_ms[FAM_PSI_COMB][choice[FAM_PSI_COMB]];
     }
+    // the TMA-fed pair of psi column passes against the classic pair (as chosen above)
+    tma_cols = 0;
+    if (tma_eligible()) {
+      const long long n = psi_n();
+      const int F3 = 3 * V;
+      C* t1 = vt12;
+      C* t2 = vt12 + (long long)F3 * n;
+      auto timed = [&](auto&& fn) {
+        fn();
+        VSAV_CUDA(cudaEventRecord(e0, st));
+        for (int k = 0; k < 3; ++k) fn();
+        VSAV_CUDA(cudaEventRecord(e1, st));
+        VSAV_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        VSAV_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        return ms / 3;
+      };
+      double ti[2], tc[2];
+      for (int v = 0; v < 2; ++v) {
+        ti[v] = timed([&]() { psi_cols_inv2_tma(vb, t1, t2, 0, F3, false, v); });
+        tc[v] = timed([&]() { psi_cols_comb_tma(t1, t2, vb, vt, 0, nullptr, nullptr, 0, F3, false, v); });
+      }
+      tma_var_inv2 = ti[1] < ti[0];
+      tma_var_comb = tc[1] < tc[0];
+      tma_ms = ti[tma_var_inv2] + tc[tma_var_comb];
+      const double classic = tune_ms[FAM_PSI_INV2][choice[FAM_PSI_INV2]] +
+                             (split_comb ? split_ms : tune_ms[FAM_PSI_COMB][choice[FAM_PSI_COMB]]);
+      tma_cols = tma_ms < classic;
+    }
     prof.on = was;
     if (getenv("VSAV_VERBOSE")) {
       const char* nm[FAM_N] = {"rows_r2c", "rows_c2r", "rows_c2c", "rows_mul", "cols", "cols_psi", "psi_inv2", "psi_comb",
@@ -1024,8 +1172,9 @@ class Solver : public SolverBase {
         for (int v = 0; v < NVAR; ++v) fprintf(stderr, "  E%d/NT%d %.3f ms", vE(v), VNT[v], tune_ms[f][v]);
         fprintf(stderr, "  -> %d\n", choice[f]);
       }
-      fprintf(stderr, "[vsav autotune %s] forward pass + combine: %s (split %.3f ms)\n",
-              std::is_same<T, double>::value ? "fp64" : "fp32", split_comb ? "split" : "fused", split_ms);
+      fprintf(stderr, "[vsav autotune %s] forward pass + combine: %s (split %.3f ms); TMA column passes: %s (%.3f ms)\n",
+              std::is_same<T, double>::value ? "fp64" : "fp32", split_comb ? "split" : "fused", split_ms,
+              tma_cols ? "on" : "off", tma_ms);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -1463,7 +1612,7 @@ class Solver : public SolverBase {
   // y = P^-1 A in (+ dots), chunk by chunk: y-inverse (2 multipliers), fused
   // x pass (inverse, x M_psi, forward), y-forward, combine
   EW dot_ew{};                 // partial layout of the dots of the last matvec
-  double split_ms = 0.0;
+  double split_ms = 0.0, tma_ms = 0.0;
   bool use_split() const { return split_comb != 0; }
   bool fused_ops = true;       // FULL form: fused column passes (VSAV_PSI_FUSED=0: separate kernels)
   void matvec(const C* in, C* out, int mode, const C* svec, bool precond = true) {
@@ -1482,6 +1631,13 @@ class Solver : public SolverBase {
       const int fc = (int)std::min<long long>(Fc, F - f0);
       C* t1 = vt12;
       C* t2 = vt12 + (long long)fc * n;
+      if (full && fused_ops && tma_cols) {
+        // the TMA-fed persistent forms of the two column passes
+        psi_cols_inv2_tma(in, t1, t2, f0, fc, true);
+        rows_mul(t1, 2LL * fc * g.Ny, full, f0, fc);
+        dot_ew.bpf = psi_cols_comb_tma(t1, t2, in, out, mode, svec, pre, f0, fc, true);
+        continue;
+      }
       if (full && fused_ops) {
         // one read of x for both inverse passes; the forward pass carries the combine
         psi_cols_inv2(in, t1, t2, f0, fc);
@@ -2001,6 +2157,12 @@ class Solver : public SolverBase {
     VSAV_CUDA(cudaMemcpyAsync(&e, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     VSAV_CUDA(cudaStreamSynchronize(st));
     s.err_flags = e;
+    if (psi32) {                                           // the FP32 helper's kernels flag into its own word
+      int e2 = 0;
+      VSAV_CUDA(cudaMemcpyAsync(&e2, psi32->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+      VSAV_CUDA(cudaStreamSynchronize(st));
+      s.err_flags |= e2;
+    }
     if (bst) {                                             // a Krylov psi solve exists (2D, or 3D variable mobility)
       int S = 3 * dm.R;
       std::vector<BiState> hb(S);

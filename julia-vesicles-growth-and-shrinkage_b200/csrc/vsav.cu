@@ -43,9 +43,13 @@ int check_status(vsav_handle* h, vsav_status* out) {
     out->psi_max_iters = s.psi_max_iters;
     out->psi_not_converged = s.psi_not_converged;
   }
-  if (s.err_flags) {
+  if (s.err_flags & 7) {
     h->err = "FATAL: W + C < 0 (flags " + std::to_string(s.err_flags) + ")";
     return VSAV_E_WC_NEGATIVE;
+  }
+  if (s.err_flags) {                // 8: a Krylov loop hit its bound; 16: a tile-copy wait timed out
+    h->err = "CUDA error: device-side bound exceeded (flags " + std::to_string(s.err_flags) + ")";
+    return VSAV_E_CUDA;
   }
   return s.psi_not_converged ? VSAV_W_NOT_CONVERGED : VSAV_OK;
 }
@@ -311,7 +315,7 @@ int vsav_get_work(vsav_handle* h, int32_t what, int32_t idx, double* out) {
 }
 int vsav_get_scalar_work(vsav_handle* h, int32_t what, double* out) {
   return guard(h, [&] {
-    if (!out || what < 0 || what > 5) throw std::runtime_error("bad scalar work id");
+    if (!out || what < 0 || what > 6) throw std::runtime_error("bad scalar work id");
     h->s->get_scalar_work(what, out);
     return VSAV_OK;
   });

@@ -6,8 +6,9 @@ pool, or code that must not call the allocator.  Its output must match
 NumPy's irfft2 of the multiplied half spectrum (FP64) to FP32 round-off and
 the handle path's irfft, on two calls in a row (the shared scratch array
 keeps the previous call's contents).  Shapes cover the smallest accepted
-transform (Nx=32, Ny=8), the longest columns (Ny=2048) and the longest rows
-(Nx=2048), and every multiplier the entry point accepts.  This file is
+transform (Nx=32, Ny=8; the handle path's FP32 transforms start at Ny=16, so
+Ny=8 is compared with NumPy alone), the longest columns (Ny=2048) and the
+longest rows (Nx=2048), and every multiplier the entry point accepts.  This file is
 collected last on purpose."""
 import math
 
@@ -37,6 +38,7 @@ def _numpy_irfft(H, mult, Lx, Ly):
 
 
 def _handle_irfft(Nx, Ny, H, mult):
+    """The handle path's FP32 irfft (its FP32 handles need Ny >= 16)."""
     from test_gpu_parity import kat_cfg
     from vsav import Handle
     h = Handle(Cfg(**kat_cfg(Nx, Ny)), precision="fp32")
@@ -46,7 +48,8 @@ def _handle_irfft(Nx, Ny, H, mult):
         h.close()
 
 
-@pytest.mark.parametrize("Nx,Ny,nf", [(32, 8, 2), (256, 128, 3), (32, 2048, 2), (2048, 8, 3)])
+@pytest.mark.parametrize("Nx,Ny,nf", [(32, 8, 2), (32, 16, 2), (256, 128, 3), (32, 2048, 2), (2048, 8, 3),
+                                      (2048, 16, 3)])
 @pytest.mark.parametrize("mult", [0, 1, 2, 4, 5])
 def test_noalloc_irfft_matches_numpy(Nx, Ny, nf, mult):
     import torch
@@ -59,8 +62,9 @@ def test_noalloc_irfft_matches_numpy(Nx, Ny, nf, mult):
     out = torch.empty((nf, Ny, Nx), dtype=torch.float32, device="cuda")
     L = 2 * math.pi
     ref = _numpy_irfft(H.astype(np.complex128), mult, L, L)
-    handle = _handle_irfft(Nx, Ny, H.astype(np.complex128), mult)
-    assert np.linalg.norm(handle - ref) / np.linalg.norm(ref) < TOL
+    handle = _handle_irfft(Nx, Ny, H.astype(np.complex128), mult) if Ny >= 16 else None
+    if handle is not None:
+        assert np.linalg.norm(handle - ref) / np.linalg.norm(ref) < TOL
     for call in range(2):                    # two calls in a row through the shared scratch
         out.fill_(float("nan"))
         rc = lib.vsav_irfft2d_f32_noalloc(spec.data_ptr(), out.data_ptr(), nf, Nx, Ny, L, L, mult, None)
@@ -70,8 +74,9 @@ def test_noalloc_irfft_matches_numpy(Nx, Ny, nf, mult):
         got = out.cpu().numpy().astype(np.float64)
         err = np.linalg.norm(got - ref) / np.linalg.norm(ref)
         assert err < TOL, (call, err)
-        err_h = np.linalg.norm(got - handle) / np.linalg.norm(handle)
-        assert err_h < TOL, (call, err_h)
+        if handle is not None:
+            err_h = np.linalg.norm(got - handle) / np.linalg.norm(handle)
+            assert err_h < TOL, (call, err_h)
 
 
 def test_noalloc_rejects_oversized_batch_and_clears_its_error():
