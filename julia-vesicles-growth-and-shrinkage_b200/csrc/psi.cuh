@@ -446,18 +446,23 @@ __device__ __forceinline__ unsigned char* tma_smem_base() {
 
 // Inverse y pass of both derivative directions (k_psi_cols_inv2, FP32):
 //   t1 = IFFT_y(i kx0 S4 x),  t2 = IFFT_y(i ky S4 x)   (x global field f0 + fl; t1/t2 chunk-local fl)
-template <int E, int NT>
+template <int E, int NT, int LOGL>
 __global__ void __launch_bounds__(NT, NT <= 512 ? 2 : 1) k_psi_cols_inv2_tma(const __grid_constant__ CUtensorMap mx, float2* __restrict__ t1,
                                                               float2* __restrict__ t2, double S4, ColArgs a, TmaTiles tt,
                                                               SysMap sm, const int* __restrict__ active, int f0,
                                                               const float2* __restrict__ tab, int* __restrict__ err) {
   using C = float2;
+  // the tile geometry is compile-time (L = 2^LOGL rows, TW = E NT / (2 L) columns), so
+  // the shared-memory index arithmetic folds to constants
+  constexpr int L = 1 << LOGL, LE = L / E, TW = E * NT / (2 * L), LOGTW = Log2<TW>::v;
+  static_assert(TW >= 2 && TW <= 16 && L >= E * E, "tile geometry");
+  constexpr int BH = L < 256 ? L : 256, NBOX = L / BH;     // rows per TMA box, boxes per column tile
   unsigned char* base = tma_smem_base();
-  const int L = 1 << a.logL, LE = L / E, TW = tt.TW;
   C* sx = reinterpret_cast<C*>(base);
   C* work = sx + (size_t)L * TW;
   uint64_t* bar = reinterpret_cast<uint64_t*>(work + col_tile_elems(L, 2 * TW, Log2<E>::v));
-  const int tid = threadIdx.x, lognl = tt.logTW + 1;
+  constexpr int lognl = LOGTW + 1;
+  const int tid = threadIdx.x;
   const int line = tid & (2 * TW - 1), i = tid >> lognl, cl = line & (TW - 1);
   const bool dir_y = line >= TW;
   const uint32_t tx = (uint32_t)((size_t)L * TW * sizeof(C));
@@ -466,7 +471,7 @@ __global__ void __launch_bounds__(NT, NT <= 512 ? 2 : 1) k_psi_cols_inv2_tma(con
   auto issue = [&](int t) {
     const int fl = t / tt.tiles, c0 = (t % tt.tiles) * TW;
     mbar_arrive_expect_tx(bar, tx);
-    for (int q = 0; q < tt.nbox; ++q) tma_load_2d(sx + (size_t)q * tt.BH * TW, &mx, c0, (f0 + fl) * a.Ny + q * tt.BH, bar);
+    for (int q = 0; q < NBOX; ++q) tma_load_2d(sx + (size_t)q * BH * TW, &mx, c0, (f0 + fl) * a.Ny + q * BH, bar);
   };
   if (tid == 0) { mbar_init(bar, 1); mbar_fence_init(); }
   __syncthreads();
@@ -495,7 +500,7 @@ __global__ void __launch_bounds__(NT, NT <= 512 ? 2 : 1) k_psi_cols_inv2_tma(con
     __syncthreads();                                          // staging consumed by every thread
     const int tn = next(t + gridDim.x);
     if (tid == 0 && tn < tt.total) { fence_proxy_async(); issue(tn); }
-    tile_fft_1buf<E, true>(v, work, lay, line, i, a.logL, lognl, tab);
+    tile_fft_1buf<E, true>(v, work, lay, line, i, LOGL, lognl, tab);
     C* o = (dir_y ? t2 : t1) + (long long)fl * a.O + c;
 #pragma unroll
     for (int j = 0; j < E; ++j) o[(long long)(i + j * LE) * a.S] = v[j];
@@ -513,25 +518,28 @@ __global__ void __launch_bounds__(NT, NT <= 512 ? 2 : 1) k_psi_cols_inv2_tma(con
 // elements by shuffle, so each computes the epilogue of E/2 rows.  Unlike
 // k_psi_cols_comb, whose epilogue runs in FP64, y is formed in FP32 (its
 // transforms are bit-identical; y differs by FP32 rounding), with the dots in FP64.
-template <int E, int NT>
-__global__ void __launch_bounds__(NT, 1) k_psi_cols_comb_tma(
+template <int E, int NT, int LOGL>
+__global__ void __launch_bounds__(NT, E * NT <= 4096 ? 2 : 1) k_psi_cols_comb_tma(
     const __grid_constant__ CUtensorMap mt1, const __grid_constant__ CUtensorMap mt2,
     const __grid_constant__ CUtensorMap mx, const __grid_constant__ CUtensorMap mc, float2* __restrict__ y, int mode,
     const double* __restrict__ adt_r, const double* __restrict__ mmax_r, double S4, ColArgs a, TmaTiles tt, SysMap sm,
     const int* __restrict__ active, int f0, const float2* __restrict__ tab, double2* __restrict__ part,
     int* __restrict__ err) {
   using C = float2;
+  constexpr int L = 1 << LOGL, LE = L / E, TW = E * NT / (2 * L), LOGTW = Log2<TW>::v;
+  static_assert(TW >= 2 && TW <= 16 && L >= E * E, "tile geometry");
+  constexpr int BH = L < 256 ? L : 256, NBOX = L / BH;     // rows per TMA box, boxes per column tile
   __shared__ double smm[2 * 4 * (NT / 32)];
   unsigned char* base = tma_smem_base();
-  const int L = 1 << a.logL, LE = L / E, TW = tt.TW;
-  const size_t tile_n = (size_t)L * TW;
+  constexpr size_t tile_n = (size_t)L * TW;
   C* s1 = reinterpret_cast<C*>(base);
   C* s2 = s1 + tile_n;
   C* sxv = s2 + tile_n;
   C* scv = sxv + tile_n;
   C* work = scv + tile_n;
   uint64_t* bar = reinterpret_cast<uint64_t*>(work + col_tile_elems(L, 2 * TW, Log2<E>::v));   // [0] t1 t2, [1] x c
-  const int tid = threadIdx.x, lognl = tt.logTW + 1;
+  constexpr int lognl = LOGTW + 1;
+  const int tid = threadIdx.x;
   const int line = tid & (2 * TW - 1), i = tid >> lognl, cl = line & (TW - 1);
   const bool is1 = line < TW;
   const uint32_t tx2 = (uint32_t)(2 * tile_n * sizeof(C));
@@ -540,17 +548,17 @@ __global__ void __launch_bounds__(NT, 1) k_psi_cols_comb_tma(
   auto issue_t = [&](int t) {
     const int fl = t / tt.tiles, c0 = (t % tt.tiles) * TW;
     mbar_arrive_expect_tx(&bar[0], tx2);
-    for (int q = 0; q < tt.nbox; ++q) {
-      tma_load_2d(s1 + (size_t)q * tt.BH * TW, &mt1, c0, fl * a.Ny + q * tt.BH, &bar[0]);
-      tma_load_2d(s2 + (size_t)q * tt.BH * TW, &mt2, c0, fl * a.Ny + q * tt.BH, &bar[0]);
+    for (int q = 0; q < NBOX; ++q) {
+      tma_load_2d(s1 + (size_t)q * BH * TW, &mt1, c0, fl * a.Ny + q * BH, &bar[0]);
+      tma_load_2d(s2 + (size_t)q * BH * TW, &mt2, c0, fl * a.Ny + q * BH, &bar[0]);
     }
   };
   auto issue_xc = [&](int t) {
     const int fl = t / tt.tiles, c0 = (t % tt.tiles) * TW;
     mbar_arrive_expect_tx(&bar[1], tx2);
-    for (int q = 0; q < tt.nbox; ++q) {
-      tma_load_2d(sxv + (size_t)q * tt.BH * TW, &mx, c0, (f0 + fl) * a.Ny + q * tt.BH, &bar[1]);
-      tma_load_2d(scv + (size_t)q * tt.BH * TW, &mc, c0, (f0 + fl) * a.Ny + q * tt.BH, &bar[1]);
+    for (int q = 0; q < NBOX; ++q) {
+      tma_load_2d(sxv + (size_t)q * BH * TW, &mx, c0, (f0 + fl) * a.Ny + q * BH, &bar[1]);
+      tma_load_2d(scv + (size_t)q * BH * TW, &mc, c0, (f0 + fl) * a.Ny + q * BH, &bar[1]);
     }
   };
   if (tid == 0) { mbar_init(&bar[0], 1); mbar_init(&bar[1], 1); mbar_fence_init(); }
@@ -573,7 +581,7 @@ __global__ void __launch_bounds__(NT, 1) k_psi_cols_comb_tma(
     __syncthreads();                                          // t1 / t2 staging consumed
     const int tn = next(t + gridDim.x);
     if (tid == 0 && tn < tt.total) { fence_proxy_async(); issue_t(tn); }
-    tile_fft_1buf<E, false>(v, work, lay, line, i, a.logL, lognl, tab);
+    tile_fft_1buf<E, false>(v, work, lay, line, i, LOGL, lognl, tab);
     // trade halves with the partner TW lanes away: the t1 holder keeps rows j < E/2,
     // the t2 holder rows j >= E/2
     constexpr int H = E / 2;
@@ -625,10 +633,22 @@ __global__ void __launch_bounds__(NT, 1) k_psi_cols_comb_tma(
         }
       }
     }
-    KSum acc[4] = {{d0, 0}, {d1, 0}, {d2, 0}, {0, 0}};
-    __syncthreads();                                          // x / c staging consumed
+    // the tile's dot partials: plain FP64 warp sums (32 terms), compensated across warps
+    double d[3] = {d0, d1, d2};
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) d[k] += __shfl_xor_sync(0xffffffffu, d[k], o);
+    const int lane = tid & 31, warp = tid >> 5;
+    if (lane == 0) { smm[warp] = d[0]; smm[NT / 32 + warp] = d[1]; smm[2 * (NT / 32) + warp] = d[2]; }
+    __syncthreads();                                          // x / c staging consumed, warp sums visible
     if (tid == 0 && tn < tt.total) { fence_proxy_async(); issue_xc(tn); }
-    block_reduce_store<4>(acc, part + ((long long)f * tt.tiles + tile) * 4, smm);
+    if (tid < 4) {
+      KSum a2{0.0, 0.0};
+      if (tid < 3)
+        for (int w = 0; w < NT / 32; ++w) a2.add(smm[tid * (NT / 32) + w]);
+      part[((long long)f * tt.tiles + tile) * 4 + tid] = make_double2(a2.s, a2.c);
+    }
     ph ^= 1;
     t = tn;
   }

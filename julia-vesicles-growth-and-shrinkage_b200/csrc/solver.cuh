@@ -538,7 +538,13 @@ class Solver : public SolverBase {
     // (graph replays included) and is what the tuning record reports
     if (const char* env = getenv("VSAV_PSI_SPLIT")) split_comb = atoi(env) != 0;
     // VSAV_PSI_TMA=0/1 overrides the choice of the TMA-fed psi column passes (where eligible)
-    if (const char* env = getenv("VSAV_PSI_TMA")) tma_cols = atoi(env) != 0 && tma_eligible();
+    if (const char* env = getenv("VSAV_PSI_TMA")) {
+      tma_cols = atoi(env) != 0 && tma_eligible();
+      for (int v = TMA_NV - 1; tma_cols && v >= 0; --v) {  // a usable variant where none was tuned
+        if (!tma_var_ok(tma_var_inv2)) tma_var_inv2 = v;
+        if (!tma_var_ok(tma_var_comb)) tma_var_comb = v;
+      }
+    }
     if constexpr (std::is_same<T, double>::value) {
       if (opt.psi_mixed && (nd == 2 || opt.psi3d_var)) {
         Options o2 = opt;
@@ -825,28 +831,35 @@ class Solver : public SolverBase {
 
   // ---- TMA-fed persistent column passes of the FULL psi operator (FP32) ----
   // One tile: TW = E * NT / (2 L) columns, t1 and t2 (or both directions) as 2 TW lines.
-  // Two block shapes with the same tile (E * NT = 8192): variant 0 E 16 / NT 512,
-  // variant 1 E 8 / NT 1024; the autotuner picks one per pass.
-  static constexpr int TMA_TILE = 8192;
-  static constexpr int TMA_VE[2] = {16, 8}, TMA_VNT[2] = {512, 1024};
+  // Two block shapes: variant 0 E 16 / NT 512 (tiles of 8192 elements: 4 columns at
+  // L = 1024, one block per SM for the combine), variant 1 E 8 / NT 512 (tiles of 4096:
+  // 2 columns, two blocks per SM); the autotuner picks one per pass.  Column lengths
+  // L = 256 .. 2048 are compiled (tma_var_ok).
+  static constexpr int TMA_NV = 2;
+  static constexpr int TMA_VE[TMA_NV] = {16, 8}, TMA_VNT[TMA_NV] = {512, 512};
   int tma_cols = 0;               // 1: the psi column passes run as the TMA-fed kernels (autotuned)
   int tma_var_inv2 = 0, tma_var_comb = 0;
-  int tma_ctas[2][2] = {{0, 0}, {0, 0}};     // [pass][variant] resident blocks (grid of the persistent launch)
+  int tma_ctas[2][TMA_NV] = {{0, 0}, {0, 0}};   // [pass][variant] resident blocks (persistent grid)
   std::map<std::pair<const void*, long long>, CUtensorMap> tmaps;
+  // variant v usable at this size: the single-buffer FFT needs L >= E^2, a tile of
+  // 2 <= TW <= 16 columns (16-byte TMA rows, lanes TW apart within a warp)
+  bool tma_var_ok(int v) const {
+    const int L = g.Ny, E = TMA_VE[v], TW = TMA_VE[v] * TMA_VNT[v] / (2 * L);
+    return L >= E * E && L >= 256 && L <= 2048 && TW >= 2 && TW <= 16 && g.Nx % TW == 0;
+  }
   bool tma_eligible() const {
     if constexpr (!std::is_same<T, float>::value) return false;
     else {
       if (g.nd != 2 || !psi_full() || vt12 == nullptr) return false;
-      const int L = g.Ny;
-      if (L < TMA_VE[0] * TMA_VE[0] || L > 4096) return false;   // the single-buffer FFT needs L >= E^2
-      const int TW = TMA_TILE / (2 * L);
-      return TW >= 2 && TW <= 16 && g.Nx % TW == 0;
+      for (int v = 0; v < TMA_NV; ++v)
+        if (tma_var_ok(v)) return true;
+      return false;
     }
   }
-  TmaTiles tma_tiles(int fc) const {
+  TmaTiles tma_tiles(int fc, int v) const {
     TmaTiles tt{};
     const int L = g.Ny;
-    tt.TW = TMA_TILE / (2 * L);
+    tt.TW = TMA_VE[v] * TMA_VNT[v] / (2 * L);
     tt.logTW = ilog2(tt.TW);
     tt.tiles = g.Nx / tt.TW;
     tt.total = fc * tt.tiles;
@@ -872,41 +885,41 @@ class Solver : public SolverBase {
     }
     return cache;
   }
-  template <int E_, int NT_>
+  template <int E_, int NT_, int LOGL>
   void launch_inv2_tma(const C* x, C* t1, C* t2, int f0, int fc, bool use_active, int var) {
     if constexpr (std::is_same<T, float>::value) {
       SysMap sm{dm.V, dm.R, d_run_of};
       long long nouter = fc;
       ColArgs a = colargs(3, nouter, E_, NT_);
-      TmaTiles tt = tma_tiles(fc);
+      TmaTiles tt = tma_tiles(fc, var);
       const size_t smem = tma_col_smem(g.Ny, tt.TW, E_, 1);
       const CUtensorMap* mx = tmap(x, 3LL * dm.V * g.Ny, tt.TW, tt.BH);
-      const int grid = std::min(tt.total, tma_grid((const void*)k_psi_cols_inv2_tma<E_, NT_>, NT_, smem, tma_ctas[0][var]));
+      const int grid = std::min(tt.total, tma_grid((const void*)k_psi_cols_inv2_tma<E_, NT_, LOGL>, NT_, smem, tma_ctas[0][var]));
       prof.begin(st);
-      k_psi_cols_inv2_tma<E_, NT_><<<grid, NT_, smem, st>>>(*mx, t1, t2, ph.S4, a, tt, sm, use_active ? bupd : nullptr, f0,
+      k_psi_cols_inv2_tma<E_, NT_, LOGL><<<grid, NT_, smem, st>>>(*mx, t1, t2, ph.S4, a, tt, sm, use_active ? bupd : nullptr, f0,
                                                              tab, d_err);
       VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
       prof.end(st, KC_COLS_F32, (double)fc * g.Pfull * 3.0 * sizeof(C));
     }
   }
-  template <int E_, int NT_>
+  template <int E_, int NT_, int LOGL>
   int launch_comb_tma(const C* t1, const C* t2, const C* x, C* y, int mode, const C* svec, const double* pre, int f0,
                       int fc, bool use_active, int var) {
     if constexpr (std::is_same<T, float>::value) {
       SysMap sm{dm.V, dm.R, d_run_of};
       long long nouter = fc;
       ColArgs a = colargs(3, nouter, E_, NT_);
-      TmaTiles tt = tma_tiles(fc);
+      TmaTiles tt = tma_tiles(fc, var);
       const size_t smem = tma_col_smem(g.Ny, tt.TW, E_, 4);
       const long long rows_g = 3LL * dm.V * g.Ny, rows_c = (long long)fc * g.Ny;
       const CUtensorMap* m1 = tmap(t1, rows_c, tt.TW, tt.BH);
       const CUtensorMap* m2 = tmap(t2, rows_c, tt.TW, tt.BH);
       const CUtensorMap* mx = tmap(x, rows_g, tt.TW, tt.BH);
       const CUtensorMap* mc = tmap(mode == 0 ? vb : svec, rows_g, tt.TW, tt.BH);
-      const int grid = std::min(tt.total, tma_grid((const void*)k_psi_cols_comb_tma<E_, NT_>, NT_, smem, tma_ctas[1][var]));
+      const int grid = std::min(tt.total, tma_grid((const void*)k_psi_cols_comb_tma<E_, NT_, LOGL>, NT_, smem, tma_ctas[1][var]));
       prof.begin(st);
-      k_psi_cols_comb_tma<E_, NT_><<<grid, NT_, smem, st>>>(*m1, *m2, *mx, *mc, y, mode, d_adt, pre, ph.S4, a, tt, sm,
+      k_psi_cols_comb_tma<E_, NT_, LOGL><<<grid, NT_, smem, st>>>(*m1, *m2, *mx, *mc, y, mode, d_adt, pre, ph.S4, a, tt, sm,
                                                              use_active ? bupd : nullptr, f0, tab, part, d_err);
       VSAV_COUNT_LAUNCH();
       VSAV_LAUNCH_CHECK();
@@ -915,16 +928,50 @@ class Solver : public SolverBase {
     }
     return 0;
   }
+  // dispatch over the compiled column lengths and block shapes (only the shapes whose
+  // tile is valid at that length are instantiated; tma_var_ok keeps the others unused)
+  template <int E_, int NT_, int LOGL>
+  static constexpr bool tma_shape_ok() {
+    constexpr int L = 1 << LOGL, TW = E_ * NT_ / (2 * L);
+    return TW >= 2 && TW <= 16 && L >= E_ * E_;
+  }
+  template <int LOGL>
+  void inv2_tma_L(const C* x, C* t1, C* t2, int f0, int fc, bool use_active, int var) {
+    if constexpr (tma_shape_ok<TMA_VE[0], TMA_VNT[0], LOGL>())
+      if (var == 0) { launch_inv2_tma<TMA_VE[0], TMA_VNT[0], LOGL>(x, t1, t2, f0, fc, use_active, 0); return; }
+    if constexpr (tma_shape_ok<TMA_VE[1], TMA_VNT[1], LOGL>())
+      if (var == 1) { launch_inv2_tma<TMA_VE[1], TMA_VNT[1], LOGL>(x, t1, t2, f0, fc, use_active, 1); return; }
+    throw std::runtime_error("TMA column pass: block shape not compiled for this column length");
+  }
+  template <int LOGL>
+  int comb_tma_L(const C* t1, const C* t2, const C* x, C* y, int mode, const C* svec, const double* pre, int f0, int fc,
+                 bool use_active, int var) {
+    if constexpr (tma_shape_ok<TMA_VE[0], TMA_VNT[0], LOGL>())
+      if (var == 0) return launch_comb_tma<TMA_VE[0], TMA_VNT[0], LOGL>(t1, t2, x, y, mode, svec, pre, f0, fc, use_active, 0);
+    if constexpr (tma_shape_ok<TMA_VE[1], TMA_VNT[1], LOGL>())
+      if (var == 1) return launch_comb_tma<TMA_VE[1], TMA_VNT[1], LOGL>(t1, t2, x, y, mode, svec, pre, f0, fc, use_active, 1);
+    throw std::runtime_error("TMA column pass: block shape not compiled for this column length");
+  }
   void psi_cols_inv2_tma(const C* x, C* t1, C* t2, int f0, int fc, bool use_active, int var = -1) {
     if (var < 0) var = tma_var_inv2;
-    if (var == 0) launch_inv2_tma<TMA_VE[0], TMA_VNT[0]>(x, t1, t2, f0, fc, use_active, 0);
-    else launch_inv2_tma<TMA_VE[1], TMA_VNT[1]>(x, t1, t2, f0, fc, use_active, 1);
+    switch (ilog2(g.Ny)) {
+      case 8: inv2_tma_L<8>(x, t1, t2, f0, fc, use_active, var); break;
+      case 9: inv2_tma_L<9>(x, t1, t2, f0, fc, use_active, var); break;
+      case 10: inv2_tma_L<10>(x, t1, t2, f0, fc, use_active, var); break;
+      case 11: inv2_tma_L<11>(x, t1, t2, f0, fc, use_active, var); break;
+      default: throw std::runtime_error("TMA column pass: unsupported column length");
+    }
   }
   int psi_cols_comb_tma(const C* t1, const C* t2, const C* x, C* y, int mode, const C* svec, const double* pre, int f0,
                         int fc, bool use_active, int var = -1) {
     if (var < 0) var = tma_var_comb;
-    if (var == 0) return launch_comb_tma<TMA_VE[0], TMA_VNT[0]>(t1, t2, x, y, mode, svec, pre, f0, fc, use_active, 0);
-    return launch_comb_tma<TMA_VE[1], TMA_VNT[1]>(t1, t2, x, y, mode, svec, pre, f0, fc, use_active, 1);
+    switch (ilog2(g.Ny)) {
+      case 8: return comb_tma_L<8>(t1, t2, x, y, mode, svec, pre, f0, fc, use_active, var);
+      case 9: return comb_tma_L<9>(t1, t2, x, y, mode, svec, pre, f0, fc, use_active, var);
+      case 10: return comb_tma_L<10>(t1, t2, x, y, mode, svec, pre, f0, fc, use_active, var);
+      case 11: return comb_tma_L<11>(t1, t2, x, y, mode, svec, pre, f0, fc, use_active, var);
+      default: throw std::runtime_error("TMA column pass: unsupported column length");
+    }
   }
 
   // time every variant of every pass family on scratch buffers; keep the fastest
@@ -1002,16 +1049,17 @@ class Solver : public SolverBase {
     }
     const char* tfile = getenv("VSAV_TUNE_FILE");
     {
+      // a tuning file that names this shape wins over the in-process cache
       std::lock_guard<std::mutex> lk(tune_mutex());
       auto it = tune_cache().find(tune_key());
-      if (it != tune_cache().end()) {
+      auto from_process = [&]() {
         for (int f = 0; f < FAM_N; ++f) choice[f] = it->second[f];
         split_comb = it->second[FAM_N];
         tma_from_code(it->second[FAM_N + 1]);
         tuned_from_cache = true;
         tune_source = "process";
-        return;
-      }
+      };
+      if (!(tfile && *tfile) && it != tune_cache().end()) { from_process(); return; }
       if (tfile && *tfile) {
         std::map<std::string, std::vector<int>> fm;
         tune_file_read(tfile, fm);
@@ -1030,12 +1078,13 @@ class Solver : public SolverBase {
           return;
         }
       }
+      if (it != tune_cache().end()) { from_process(); return; }
     }
     autotune_measure();
     std::lock_guard<std::mutex> lk(tune_mutex());
     std::vector<int> c(choice, choice + FAM_N);
     c.push_back(split_comb);
-    c.push_back(tma_cols | tma_var_inv2 << 1 | tma_var_comb << 2);
+    c.push_back(tma_cols | tma_var_inv2 << 1 | tma_var_comb << 3);
     tune_cache()[tune_key()] = c;
     if (tfile && *tfile) {
       std::map<std::string, std::vector<int>> fm;
@@ -1045,9 +1094,10 @@ class Solver : public SolverBase {
     }
   }
   void tma_from_code(int code) {
-    tma_cols = (code & 1) && tma_eligible();
-    tma_var_inv2 = (code >> 1) & 1;
-    tma_var_comb = (code >> 2) & 1;
+    tma_var_inv2 = (code >> 1) & 3;
+    tma_var_comb = (code >> 3) & 3;
+    if (tma_var_inv2 >= TMA_NV || tma_var_comb >= TMA_NV) tma_var_inv2 = tma_var_comb = 0;
+    tma_cols = (code & 1) && tma_eligible() && tma_var_ok(tma_var_inv2) && tma_var_ok(tma_var_comb);
   }
   // the variants in use, as JSON: {"key", "source", "split", families: "E<e>/NT<nt>"}
   std::string tuning_json() const {
@@ -1150,13 +1200,15 @@ class Solver : public SolverBase {
         VSAV_CUDA(cudaEventElapsedTime(&ms, e0, e1));
         return ms / 3;
       };
-      double ti[2], tc[2];
-      for (int v = 0; v < 2; ++v) {
+      double ti[TMA_NV], tc[TMA_NV];
+      tma_var_inv2 = tma_var_comb = -1;
+      for (int v = 0; v < TMA_NV; ++v) {
+        if (!tma_var_ok(v)) continue;
         ti[v] = timed([&]() { psi_cols_inv2_tma(vb, t1, t2, 0, F3, false, v); });
         tc[v] = timed([&]() { psi_cols_comb_tma(t1, t2, vb, vt, 0, nullptr, nullptr, 0, F3, false, v); });
+        if (tma_var_inv2 < 0 || ti[v] < ti[tma_var_inv2]) tma_var_inv2 = v;
+        if (tma_var_comb < 0 || tc[v] < tc[tma_var_comb]) tma_var_comb = v;
       }
-      tma_var_inv2 = ti[1] < ti[0];
-      tma_var_comb = tc[1] < tc[0];
       tma_ms = ti[tma_var_inv2] + tc[tma_var_comb];
       const double classic = tune_ms[FAM_PSI_INV2][choice[FAM_PSI_INV2]] +
                              (split_comb ? split_ms : tune_ms[FAM_PSI_COMB][choice[FAM_PSI_COMB]]);

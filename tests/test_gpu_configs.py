@@ -196,3 +196,30 @@ def test_mixed_both_column_pass_forms(tma, monkeypatch):
     assert max(err.values()) < 1e-5, err
     assert np.max(h.true_residuals()) < 1e-8 * 1.05, h.true_residuals()
     h.close()
+
+
+@pytest.mark.parametrize("var", [0, 1])
+def test_tma_tile_shapes(var, tmp_path, monkeypatch):
+    """Each block shape of the TMA-fed column passes (0: E 16 / 512 threads,
+    1: E 8 / 512 with half-width tiles), pinned through a tuning file: the mixed
+    path reproduces the oracle at 512^2 x 4 within its bar."""
+    import json as js
+    from vsav import Handle
+    key = "4:512x512x1:V4:R1:f0"               # the FP32 psi helper of this configuration
+    code = 1 | var << 1 | var << 3             # TMA on, both passes in shape `var`
+    path = tmp_path / "tune.json"
+    path.write_text(js.dumps({key: [0] * 9 + [0, code]}))
+    monkeypatch.setenv("VSAV_TUNE_FILE", str(path))
+    kw, meta, g = load("cfg_multi2d_512x4")
+    phi, psi = initial(meta, kw)
+    h = Handle(Cfg(**kw), precision="mixed", psi_rtol=1e-8, psi_stop="true", psi_check=True)
+    t = h.tuning()["psi_fp32"]
+    assert t["source"] == "file" and t["psi_column_passes"] == "tma", t
+    shape = {0: "E16/NT512", 1: "E8/NT512"}[var]
+    assert t["variants"]["psi_inv2_tma"] == shape and t["variants"]["psi_comb_tma"] == shape, t
+    h.init_state(phi, psi)
+    E, A = h.run(1, meta["steps"], monitor=True)
+    err = field_errors(h, g, meta)
+    assert max(err.values()) < 1e-5, err
+    assert np.max(h.true_residuals()) < 1e-8 * 1.05, h.true_residuals()
+    h.close()
