@@ -17,7 +17,7 @@ OUT = os.path.join(HERE, "vsav", "libvsav.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "-Xcompiler", "-fPIC", "-diag-suppress", "177"]
-UNITS = ("vsav.cu", "net.cu", "noalloc.cu")
+UNITS = ("vsav.cu", "solver_f32.cu", "solver_f64.cu", "net.cu", "noalloc.cu")
 
 
 def sources():

@@ -318,7 +318,7 @@ __device__ __forceinline__ void smem_passes_1buf(C* buf, const Lay lay, int logL
 // thread of the block holding one butterfly (a full tile).
 template <int E, bool INV, typename C, typename Lay>
 __device__ __forceinline__ void tile_fft_1buf(C (&v)[E], C* buf, const Lay lay, int line, int i, int logL, int lognl,
-                                              const C* __restrict__ tab) {
+                                              const C* __restrict__ tab, const C* twx = nullptr) {
   constexpr int LOGE = Log2<E>::v;
   const int LE = 1 << (logL - LOGE);
   dft_reg<E, INV>(v);
@@ -328,12 +328,17 @@ __device__ __forceinline__ void tile_fft_1buf(C (&v)[E], C* buf, const Lay lay, 
   smem_passes_1buf<E, INV>(buf, lay, logL, lognl, E, logL - 2 * LOGE, tab);
 #pragma unroll
   for (int r = 0; r < E; ++r) v[r] = buf[lay(line, i + r * LE)];
+  // twiddles of the last pass: exp(-+2 pi i m / L), from the table row of length L in
+  // global memory, or from a per-butterfly table the caller staged in shared memory
+  // (tw_last_table: twx[(q - 1) LE + i] = w^(q i), q = 1..3, then twx[(q + 2) LE + i] =
+  // w^(4 q i), q = 1..E/4-1, so consecutive butterflies read consecutive words)
+  const int LEv = 1 << (logL - LOGE);
   if constexpr (E >= 16) {
     C lo[4], hi[E / 4];
 #pragma unroll
-    for (int q = 1; q < 4; ++q) { lo[q] = __ldg(&tab[(1 << logL) + q * i]); if (INV) lo[q].y = -lo[q].y; }
+    for (int q = 1; q < 4; ++q) { lo[q] = twx ? twx[(q - 1) * LEv + i] : __ldg(&tab[(1 << logL) + q * i]); if (INV) lo[q].y = -lo[q].y; }
 #pragma unroll
-    for (int q = 1; q < E / 4; ++q) { hi[q] = __ldg(&tab[(1 << logL) + 4 * q * i]); if (INV) hi[q].y = -hi[q].y; }
+    for (int q = 1; q < E / 4; ++q) { hi[q] = twx ? twx[(q + 2) * LEv + i] : __ldg(&tab[(1 << logL) + 4 * q * i]); if (INV) hi[q].y = -hi[q].y; }
 #pragma unroll
     for (int r = 1; r < E; ++r) {
       C w = (r & 3) == 0 ? hi[r >> 2] : ((r >> 2) == 0 ? lo[r & 3] : hi[r >> 2] * lo[r & 3]);
@@ -342,13 +347,41 @@ __device__ __forceinline__ void tile_fft_1buf(C (&v)[E], C* buf, const Lay lay, 
   } else {
 #pragma unroll
     for (int r = 1; r < E; ++r) {
-      C w = __ldg(&tab[(1 << logL) + r * i]);
+      C w = twx ? twx[(r - 1) * LEv + i] : __ldg(&tab[(1 << logL) + r * i]);
       if (INV) w.y = -w.y;
       v[r] = v[r] * w;
     }
   }
   dft_reg<E, INV>(v);
 }
+
+// the per-butterfly twiddle table of tile_fft_1buf's last pass (twx), built by the
+// block from the global table: entries of the row exp(-2 pi i m / L)
+template <int E>
+__host__ __device__ constexpr int tw_last_rows() { return E >= 16 ? 3 + E / 4 - 1 : E - 1; }
+template <int E, typename C>
+__device__ __forceinline__ void tw_last_table(C* twx, int logL, const C* __restrict__ tab) {
+  constexpr int LOGE = Log2<E>::v, NR = tw_last_rows<E>();
+  const int L = 1 << logL, LE = 1 << (logL - LOGE);
+  for (int k = threadIdx.x; k < NR * LE; k += blockDim.x) {
+    const int q = k / LE, i = k - q * LE;
+    int m;
+    if (E >= 16) m = (q < 3) ? (q + 1) * i : 4 * (q - 2) * i;
+    else m = (q + 1) * i;
+    twx[k] = tab[L + m];
+  }
+}
+
+// row layout with one pad slot every 2^SH elements (SH = log2 of the register radix,
+// so the stride-E writes after the first register pass spread over all banks) and an
+// odd shift per line
+template <int SH>
+struct RowLayP {
+  int LP;
+  __device__ __forceinline__ int operator()(int line, int e) const { return line * LP + e + (e >> SH); }
+  static constexpr bool line_fast = false;
+  static __host__ __device__ constexpr int pitch(int L) { return L + (L >> SH) + 1; }
+};
 
 // minimum resident CTAs that the register budget must allow, per (E, NT)
 template <int E, int NT> struct MinB {

@@ -50,7 +50,7 @@ __device__ __forceinline__ void ew_store_partials(KSum (&acc)[K], double2* part,
 }
 
 // per-field totals: out[f*K + k] = sum over blocks of field f (compensated)
-__global__ void k_fin_fields(const double2* __restrict__ part, int bpf, int K, double* __restrict__ out) {
+static __global__ void k_fin_fields(const double2* __restrict__ part, int bpf, int K, double* __restrict__ out) {
   const int f = blockIdx.x;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int k = warp; k < K; k += nw) {
@@ -70,7 +70,7 @@ __global__ void k_fin_fields(const double2* __restrict__ part, int bpf, int K, d
 }
 
 // per-field maxima (partials hold max in .x)
-__global__ void k_fin_max(const double2* __restrict__ part, int bpf, int K, int k0, double* __restrict__ out) {
+static __global__ void k_fin_max(const double2* __restrict__ part, int bpf, int K, int k0, double* __restrict__ out) {
   const int f = blockIdx.x;
   double m = -INFINITY;
   for (int b = threadIdx.x; b < bpf; b += blockDim.x) m = fmax(m, part[((long long)f * bpf + b) * K + k0].x);
@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(256) k_area(const T* __restrict__ phi, const T
 //  asum[v] = f_surf sums, fs[v*3+1..2] = (f_bend, E2) sums, fo[v*3+1..2] = (f_osm, psi^2) sums,
 //  Mmax_v[v] = block maxima.  Writes sc[r*8 + 0..7] = (R1s, R2s, R3s, Mmax, W1, W2, W3, -)
 //  and factor[v], area[v].  err |= 1/2/4 when W_i + C_i < 0.
-__global__ void k_fin_H(const double* __restrict__ asum, const double* __restrict__ fs, const double* __restrict__ fo,
+static __global__ void k_fin_H(const double* __restrict__ asum, const double* __restrict__ fs, const double* __restrict__ fo,
                         const double* __restrict__ mmax_v, const double* __restrict__ A0, Phys ph, Runs rn, double* __restrict__ sc,
                         double* __restrict__ factor, double* __restrict__ area, int* __restrict__ err) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
@@ -449,7 +449,7 @@ __device__ inline void solve3(double A[3][3], double bb[3], double x[3]) {
 
 // Step 2 scalar solve per run.  scp/sco: [R][4] (Q,R1,R2,R3) present/old.
 // out r2[r*6 + 0..5] = R11 R21 R31 R12 R22 R32
-__global__ void k_fin_step2(const double* __restrict__ fd, const double* __restrict__ scp, const double* __restrict__ sco,
+static __global__ void k_fin_step2(const double* __restrict__ fd, const double* __restrict__ scp, const double* __restrict__ sco,
                             double a, double b, double c, Phys ph, Runs rn, double* __restrict__ r2) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= rn.R) return;
@@ -588,7 +588,7 @@ __global__ void __launch_bounds__(256) k_dot5r(const T* __restrict__ coupl, cons
 }
 
 // Step 5 scalar (Solvers.jl:407-420).  Writes Q into qv[r], theta into th[2r..]
-__global__ void k_fin_step5(const double* __restrict__ fv, const double* __restrict__ fr, const double* __restrict__ scp,
+static __global__ void k_fin_step5(const double* __restrict__ fv, const double* __restrict__ fr, const double* __restrict__ scp,
                             const double* __restrict__ sco, const double* __restrict__ dtv, int use_conf_dt,
                             double a, double b, double c, Phys ph, Runs rn, double* __restrict__ qv, double* __restrict__ th) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
@@ -627,7 +627,7 @@ __global__ void k_step6(const cplx<T>* __restrict__ s3, const double* __restrict
     }
   }
 }
-__global__ void k_step6_scalars(const double* __restrict__ r2, const double* __restrict__ qv, double* __restrict__ scn, int R) {
+static __global__ void k_step6_scalars(const double* __restrict__ r2, const double* __restrict__ qv, double* __restrict__ scn, int R) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= R) return;
   double Q = qv[r];
@@ -743,7 +743,7 @@ __global__ void __launch_bounds__(256) k_mon_r(const T* __restrict__ up, const T
   }
   ew_store_partials<3>(acc, part, ew, sm);
 }
-__global__ void k_fin_mon(const double* __restrict__ fv, const double* __restrict__ fr, const double* __restrict__ scp,
+static __global__ void k_fin_mon(const double* __restrict__ fv, const double* __restrict__ fr, const double* __restrict__ scp,
                           const double* __restrict__ sco, const double* __restrict__ dtv, const double* __restrict__ A0,
                           Phys ph, Runs rn, double* __restrict__ energy, double* __restrict__ aratio, double* __restrict__ area) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;

@@ -654,6 +654,118 @@ __global__ void __launch_bounds__(NT, E * NT <= 4096 ? 2 : 1) k_psi_cols_comb_tm
   }
 }
 
+// ---------------------------------------------------------------------------
+// The FULL x pass of the operator (k_rows_mul, FP32) as a persistent pipeline fed
+// by bulk copies.  A tile is NL = NT E / L consecutive rows of one plane (t1 or t2
+// of one field) -- one contiguous block of NL L complex floats -- with the NL rows
+// of M_psi it needs.  One thread moves both into a ring of S shared-memory slots by
+// cp.async.bulk, completed on the slot's mbarrier; the block transforms the tile in
+// its slot (the rows are read into registers, then the slot is the padded exchange
+// of both transforms), writes the result back into the slot and one thread stores
+// it with a bulk copy, so the loads of the next tiles and the store of the last one
+// run on the copy engine while a tile is transformed.  The tiles of a row group are
+// ordered plane-fastest (t1 and t2 of field 0, then of field 1, ...), so the M_psi
+// rows of a group are read from HBM once and reused from L2 by the other planes.
+// The butterflies, twiddles and radix split are those of the ping-pong kernel, so
+// the results are bit-identical to k_rows_mul<float, E, *, true>.
+//   t rows: [2][fc][Ny][L] (t1 | t2 of the chunk's fields f0 .. f0+fc-1).
+// Waits on the mbarriers are bounded (tma.cuh): a copy that never lands sets the
+// error word and every thread of the block returns.
+// ---------------------------------------------------------------------------
+template <int E, int NT, int LOGL, int S>
+struct BulkRows {
+  static constexpr int L = 1 << LOGL, LE = L / E, NL = NT * E / L, LOGE = Log2<E>::v;
+  static constexpr int LP = RowLayP<LOGE>::pitch(L);            // padded line of the in-slot exchange
+  static constexpr size_t t_elems = ((size_t)NL * LP + 1) / 2 * 2; // complex slots of a ring entry's tile part (16-B multiple)
+  static constexpr uint32_t TB = NL * L * 8, MB = NL * L * 4;    // bytes copied per tile: t rows, M rows
+  static constexpr size_t slot_bytes = t_elems * 8 + MB;
+  static constexpr size_t tw_bytes = (size_t)tw_last_rows<E>() * LE * 8;
+  static constexpr size_t smem = 1024 + S * slot_bytes + tw_bytes + 8 * S;
+  static constexpr bool ok = NL >= 1 && L >= E * E && NT % 32 == 0 && S >= 2;
+};
+
+template <int E, int NT, int LOGL, int S>
+__global__ void __launch_bounds__(NT, 2) k_rows_mul_bulk(float2* __restrict__ t, const float* __restrict__ M, float scale,
+                                                         int Ny, int fc, int f0, long long ntiles, SysMap sm,
+                                                         const int* __restrict__ active, const float2* __restrict__ tab,
+                                                         int* __restrict__ err) {
+  using C = float2;
+  using G = BulkRows<E, NT, LOGL, S>;
+  constexpr int L = G::L, LE = G::LE, NL = G::NL, LOGNL = Log2<NL>::v;
+  static_assert(G::ok, "tile geometry");
+  unsigned char* base = tma_smem_base();
+  // ring entry s: the tile's t rows (landing unpadded, then the padded exchange of both
+  // transforms, then the result) followed by its M rows
+  auto tslot = [&](int s_) { return reinterpret_cast<C*>(base + (size_t)s_ * G::slot_bytes); };
+  auto mslot = [&](int s_) { return reinterpret_cast<float*>(base + (size_t)s_ * G::slot_bytes + G::t_elems * 8); };
+  C* twx = reinterpret_cast<C*>(base + S * G::slot_bytes);        // twiddles of the last pass, per butterfly
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base + S * G::slot_bytes + G::tw_bytes);
+  const int tid = threadIdx.x;
+  int line, i;
+  row_owner<E>(LOGL, line, i);
+  const int planes = 2 * fc;
+  // tile tau: plane p = tau % planes (t1/t2 of chunk field p / 2), row group tau / planes
+  auto act = [&](long long tau) { return !active || active[sm.sys(f0 + (int)(tau % planes) / 2)]; };
+  auto next = [&](long long tau) { while (tau < ntiles && !act(tau)) tau += gridDim.x; return tau; };
+  auto row_of = [&](long long tau) {
+    const int p = (int)(tau % planes), rg = (int)(tau / planes);
+    return ((long long)(p & 1) * fc + (p >> 1)) * Ny + (long long)rg * NL;
+  };
+  auto issue = [&](long long tau, int s_) {
+    const long long row = row_of(tau);
+    const int field = f0 + (int)(tau % planes) / 2;
+    const long long mrow = (long long)(field % sm.V) * Ny + row % Ny;
+    mbar_arrive_expect_tx(&bar[s_], G::TB + G::MB);
+    bulk_load(tslot(s_), t + row * L, G::TB, &bar[s_]);
+    bulk_load(mslot(s_), M + mrow * L, G::MB, &bar[s_]);
+  };
+  tw_last_table<E>(twx, LOGL, tab);
+  if (tid == 0) {
+    for (int s_ = 0; s_ < S; ++s_) mbar_init(&bar[s_], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  long long cur = next(blockIdx.x);
+  long long ld = cur;                       // thread 0: the next tile to load
+  if (tid == 0)
+    for (int s_ = 0; s_ < S && ld < ntiles; ++s_) { issue(ld, s_); ld = next(ld + gridDim.x); }
+  const RowLayP<G::LOGE> lay{G::LP};
+  for (int k = 0; cur < ntiles; ++k) {
+    const int s_ = k % S;
+    const long long row = row_of(cur);
+    const bool ok = mbar_wait(&bar[s_], (uint32_t)((k / S) & 1), err);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) bulk_wait_all();
+      return;
+    }
+    C* ts = tslot(s_);
+    C v[E];
+#pragma unroll
+    for (int j = 0; j < E; ++j) v[j] = ts[(size_t)line * L + i + j * LE];
+    __syncthreads();                                          // the landed rows are consumed: the slot is the exchange
+    // the slot of the previous tile: its bulk store has had this tile's wait to read it; refill
+    if (tid == 0 && k > 0 && ld < ntiles) {
+      bulk_wait_read_all();
+      issue(ld, (k + S - 1) % S);
+      ld = next(ld + gridDim.x);
+    }
+    tile_fft_1buf<E, true>(v, ts, lay, line, i, LOGL, LOGNL, tab, twx);
+    const float* ms = mslot(s_) + (size_t)line * L + i;
+#pragma unroll
+    for (int j = 0; j < E; ++j) { const float mv = ms[j * LE] * scale; v[j].x *= mv; v[j].y *= mv; }
+    __syncthreads();                                          // exchange reused by the forward transform
+    tile_fft_1buf<E, false>(v, ts, lay, line, i, LOGL, LOGNL, tab, twx);
+    __syncthreads();                                          // every exchange read done: the slot takes the result
+#pragma unroll
+    for (int j = 0; j < E; ++j) ts[(size_t)line * L + i + j * LE] = v[j];
+    fence_proxy_async();
+    __syncthreads();
+    if (tid == 0) { bulk_store(t + row * L, ts, G::TB); bulk_commit(); }
+    cur = next(cur + gridDim.x);
+  }
+  if (tid == 0) bulk_wait_all();
+}
+
 // The 3D full-spectrum operator output (the 2D FULL form with a z direction):
 //   y = P^-1 ( a_dt x - (i kx0 t1 + i ky t2 + i kz t3) ),  P^-1 = 1/(a_dt + Mmax S4 k^2) or 1,
 // with k_psi_combine's modes and dot products.  t1..t3 hold F fields each.
@@ -832,6 +944,7 @@ __global__ void __launch_bounds__(256) k_psi_init(const cplx<T>* __restrict__ b,
   const int rr = sm.run_of[f % sm.V];
   const double adt = adt_r[rr], mm = mmax_r ? mmax_r[rr] : 0.0;
   const long long beg = (long long)blockIdx.x * ew.chunk, end = min(ew.n, beg + ew.chunk);
+#pragma unroll 4
   for (long long s = beg + threadIdx.x; s < end; s += blockDim.x) {
     int kx, ky; double kxv, kyv, w;
     vk(g, s, kx, ky, kxv, kyv, w);
@@ -852,20 +965,33 @@ __global__ void __launch_bounds__(256) k_psi_init(const cplx<T>* __restrict__ b,
   block_reduce_store<4>(acc, part + ((long long)blockIdx.y * ew.bpf + blockIdx.x) * 4, smm);
 }
 
-// s = r - alpha v
+// s = r - alpha v.  Each thread loads VB slots of both operands before it
+// computes, so several loads per thread are in flight.
+constexpr int VB = 4;
 template <typename T>
-__global__ void k_psi_s(const cplx<T>* __restrict__ r, const cplx<T>* __restrict__ v, cplx<T>* __restrict__ s,
-                        const BiState* __restrict__ st, SysMap sm, EW ew) {
+__global__ void __launch_bounds__(256) k_psi_s(const cplx<T>* __restrict__ r, const cplx<T>* __restrict__ v,
+                                               cplx<T>* __restrict__ s, const BiState* __restrict__ st, SysMap sm, EW ew) {
   const BiState& b = st[sm.sys(blockIdx.y)];
   if (!b.active) return;
   const double2 a = b.alpha;
-  EW_LOOP(ew, f, q) {
-    long long i = (long long)f * ew.n + q;
-    cplx<T> rv = r[i], vv = v[i];
-    cplx<T> o;
-    o.x = (double)rv.x - (a.x * (double)vv.x - a.y * (double)vv.y);
-    o.y = (double)rv.y - (a.x * (double)vv.y + a.y * (double)vv.x);
-    s[i] = o;
+  const long long base = (long long)blockIdx.y * ew.n;
+  const long long q0 = (long long)blockIdx.x * ew.chunk, q1 = min(ew.n, q0 + ew.chunk);
+  for (long long qb = q0 + threadIdx.x; qb < q1; qb += VB * blockDim.x) {
+    cplx<T> rv[VB], vv[VB];
+#pragma unroll
+    for (int u = 0; u < VB; ++u) {
+      const long long q = qb + (long long)u * blockDim.x;
+      if (q < q1) { rv[u] = r[base + q]; vv[u] = v[base + q]; }
+    }
+#pragma unroll
+    for (int u = 0; u < VB; ++u) {
+      const long long q = qb + (long long)u * blockDim.x;
+      if (q >= q1) break;
+      cplx<T> o;
+      o.x = (double)rv[u].x - (a.x * (double)vv[u].x - a.y * (double)vv[u].y);
+      o.y = (double)rv[u].y - (a.x * (double)vv[u].y + a.y * (double)vv[u].x);
+      s[base + q] = o;
+    }
   }
 }
 
@@ -876,7 +1002,7 @@ __global__ void k_psi_s(const cplx<T>* __restrict__ r, const cplx<T>* __restrict
 // left-preconditioned form r = M^-1 (b - A x), so ||D r|| is the norm of the true
 // residual b - A x, at no extra pass (mmax_r == nullptr: D = 1, r is already true).
 template <typename T>
-__global__ void __launch_bounds__(256) k_psi_update(cplx<T>* __restrict__ x, cplx<T>* __restrict__ r, const cplx<T>* __restrict__ p,
+__global__ void __launch_bounds__(256, 2) k_psi_update(cplx<T>* __restrict__ x, cplx<T>* __restrict__ r, const cplx<T>* __restrict__ p,
                                                     const cplx<T>* __restrict__ s, const cplx<T>* __restrict__ t,
                                                     const cplx<T>* __restrict__ cvec, const BiState* __restrict__ st,
                                                     VGeom g, SysMap sm, EW ew, double2* part,
@@ -890,36 +1016,52 @@ __global__ void __launch_bounds__(256) k_psi_update(cplx<T>* __restrict__ x, cpl
     const double2 al = b.alpha, om = b.omega;
     const int run = sm.run_of[f % sm.V];
     const double adt = mmax_r ? adt_r[run] : 0.0, mm = mmax_r ? mmax_r[run] : 0.0;
+    const long long base = (long long)f * g.n;
     const long long beg = (long long)blockIdx.x * ew.chunk, end = min(ew.n, beg + ew.chunk);
-    for (long long q = beg + threadIdx.x; q < end; q += blockDim.x) {
-      int kx, ky; double kxv, kyv, w;
-      vk(g, q, kx, ky, kxv, kyv, w);
-      if (w == 0.0) continue;
-      long long j = (long long)f * g.n + q;
-      cplx<T> xv = x[j], pv = p[j], sv = s[j], tv = t[j];
-      const cplx<T> hv = shat ? shat[j] : sv;
-      cplx<T> xa;
-      xa.x = (double)xv.x + (al.x * (double)pv.x - al.y * (double)pv.y);
-      xa.y = (double)xv.y + (al.x * (double)pv.y + al.y * (double)pv.x);
-      cplx<T> xn;
-      xn.x = (double)xa.x + (om.x * (double)hv.x - om.y * (double)hv.y);
-      xn.y = (double)xa.y + (om.x * (double)hv.y + om.y * (double)hv.x);
-      x[j] = xn;
-      cplx<T> rn;
-      rn.x = (double)sv.x - (om.x * (double)tv.x - om.y * (double)tv.y);
-      rn.y = (double)sv.y - (om.x * (double)tv.y + om.y * (double)tv.x);
-      r[j] = rn;
-      cplx<T> c = cvec[j];
-      acc[0].add(w * ((double)c.x * (double)rn.x + (double)c.y * (double)rn.y));
-      if (g.full) acc[1].add((double)c.x * (double)rn.y - (double)c.y * (double)rn.x);
-      const double rr = (double)rn.x * (double)rn.x + (double)rn.y * (double)rn.y;
-      acc[2].add(w * rr);
-      double dd = 1.0;
-      if (mmax_r) {
-        const double kxp = (!g.full && kx == g.Nx / 2) ? 0.0 : kxv;
-        dd = adt + mm * S4 * (kxp * kxp + kyv * kyv + vk_kz2(g, q));
+    // VB slots per thread per round: every operand of the round is loaded before any
+    // arithmetic, so the loads are in flight together
+    for (long long qb = beg + threadIdx.x; qb < end; qb += VB * blockDim.x) {
+      cplx<T> xv[VB], pv[VB], sv[VB], tv[VB], hv[VB], cv[VB];
+#pragma unroll
+      for (int u = 0; u < VB; ++u) {
+        const long long q = qb + (long long)u * blockDim.x;
+        if (q < end) {
+          const long long j = base + q;
+          xv[u] = x[j]; pv[u] = p[j]; sv[u] = s[j]; tv[u] = t[j]; cv[u] = cvec[j];
+          hv[u] = shat ? shat[j] : sv[u];
+        }
       }
-      acc[3].add(w * dd * dd * rr);
+#pragma unroll
+      for (int u = 0; u < VB; ++u) {
+        const long long q = qb + (long long)u * blockDim.x;
+        if (q >= end) break;
+        int kx, ky; double kxv, kyv, w;
+        vk(g, q, kx, ky, kxv, kyv, w);
+        if (w == 0.0) continue;
+        const long long j = base + q;
+        cplx<T> xa;
+        xa.x = (double)xv[u].x + (al.x * (double)pv[u].x - al.y * (double)pv[u].y);
+        xa.y = (double)xv[u].y + (al.x * (double)pv[u].y + al.y * (double)pv[u].x);
+        cplx<T> xn;
+        xn.x = (double)xa.x + (om.x * (double)hv[u].x - om.y * (double)hv[u].y);
+        xn.y = (double)xa.y + (om.x * (double)hv[u].y + om.y * (double)hv[u].x);
+        x[j] = xn;
+        cplx<T> rn;
+        rn.x = (double)sv[u].x - (om.x * (double)tv[u].x - om.y * (double)tv[u].y);
+        rn.y = (double)sv[u].y - (om.x * (double)tv[u].y + om.y * (double)tv[u].x);
+        r[j] = rn;
+        const cplx<T> c = cv[u];
+        acc[0].add(w * ((double)c.x * (double)rn.x + (double)c.y * (double)rn.y));
+        if (g.full) acc[1].add((double)c.x * (double)rn.y - (double)c.y * (double)rn.x);
+        const double rr = (double)rn.x * (double)rn.x + (double)rn.y * (double)rn.y;
+        acc[2].add(w * rr);
+        double dd = 1.0;
+        if (mmax_r) {
+          const double kxp = (!g.full && kx == g.Nx / 2) ? 0.0 : kxv;
+          dd = adt + mm * S4 * (kxp * kxp + kyv * kyv + vk_kz2(g, q));
+        }
+        acc[3].add(w * dd * dd * rr);
+      }
     }
   }
   block_reduce_store<4>(acc, part + ((long long)blockIdx.y * ew.bpf + blockIdx.x) * 4, smm);
@@ -927,20 +1069,32 @@ __global__ void __launch_bounds__(256) k_psi_update(cplx<T>* __restrict__ x, cpl
 
 // p = r + beta (p - omega v)   (only systems that were active in this iteration: flag `upd`)
 template <typename T>
-__global__ void k_psi_p(cplx<T>* __restrict__ p, const cplx<T>* __restrict__ r, const cplx<T>* __restrict__ v,
-                        const BiState* __restrict__ st, const int* __restrict__ upd, SysMap sm, EW ew) {
+__global__ void __launch_bounds__(256) k_psi_p(cplx<T>* __restrict__ p, const cplx<T>* __restrict__ r,
+                                               const cplx<T>* __restrict__ v, const BiState* __restrict__ st,
+                                               const int* __restrict__ upd, SysMap sm, EW ew) {
   const int sy = sm.sys(blockIdx.y);
   if (!upd[sy]) return;
   const double2 be = st[sy].beta, om = st[sy].omega;
-  EW_LOOP(ew, f, q) {
-    long long i = (long long)f * ew.n + q;
-    cplx<T> pv = p[i], rv = r[i], vv = v[i];
-    double ax = (double)pv.x - (om.x * (double)vv.x - om.y * (double)vv.y);
-    double ay = (double)pv.y - (om.x * (double)vv.y + om.y * (double)vv.x);
-    cplx<T> o;
-    o.x = (double)rv.x + (be.x * ax - be.y * ay);
-    o.y = (double)rv.y + (be.x * ay + be.y * ax);
-    p[i] = o;
+  const long long base = (long long)blockIdx.y * ew.n;
+  const long long q0 = (long long)blockIdx.x * ew.chunk, q1 = min(ew.n, q0 + ew.chunk);
+  for (long long qb = q0 + threadIdx.x; qb < q1; qb += VB * blockDim.x) {
+    cplx<T> pv[VB], rv[VB], vv[VB];
+#pragma unroll
+    for (int u = 0; u < VB; ++u) {
+      const long long q = qb + (long long)u * blockDim.x;
+      if (q < q1) { pv[u] = p[base + q]; rv[u] = r[base + q]; vv[u] = v[base + q]; }
+    }
+#pragma unroll
+    for (int u = 0; u < VB; ++u) {
+      const long long q = qb + (long long)u * blockDim.x;
+      if (q >= q1) break;
+      const double ax = (double)pv[u].x - (om.x * (double)vv[u].x - om.y * (double)vv[u].y);
+      const double ay = (double)pv[u].y - (om.x * (double)vv[u].y + om.y * (double)vv[u].x);
+      cplx<T> o;
+      o.x = (double)rv[u].x + (be.x * ax - be.y * ay);
+      o.y = (double)rv[u].y + (be.x * ay + be.y * ax);
+      p[base + q] = o;
+    }
   }
 }
 
@@ -963,7 +1117,7 @@ __device__ __forceinline__ void sys_sums(const double* fd, int sy, const SysMap&
 
 // stop_true: stop on the true residual ||b - A x|| <= atol + rtol ||b|| (slot 3 of the
 // dots) instead of Krylov.jl's preconditioned ||M^-1 r|| <= atol + rtol ||M^-1 b|| (slot 2)
-__global__ void k_bi_init(const double* __restrict__ fd, BiState* __restrict__ st, int* __restrict__ upd, SysMap sm, int S, int F,
+static __global__ void k_bi_init(const double* __restrict__ fd, BiState* __restrict__ st, int* __restrict__ upd, SysMap sm, int S, int F,
                           double atol, double rtol, int itmax, int stop_true) {
   int sy = blockIdx.x * blockDim.x + threadIdx.x;
   if (sy >= S) return;
@@ -985,21 +1139,21 @@ __global__ void k_bi_init(const double* __restrict__ fd, BiState* __restrict__ s
   st[sy] = b;
   upd[sy] = b.active;
 }
-__global__ void k_bi_alpha(const double* __restrict__ fd, BiState* __restrict__ st, SysMap sm, int S, int F) {
+static __global__ void k_bi_alpha(const double* __restrict__ fd, BiState* __restrict__ st, SysMap sm, int S, int F) {
   int sy = blockIdx.x * blockDim.x + threadIdx.x;
   if (sy >= S || !st[sy].active) return;
   double d[4];
   sys_sums(fd, sy, sm, F, d);
   st[sy].alpha = cdiv(st[sy].rho, make_double2(d[0], d[1]));
 }
-__global__ void k_bi_omega(const double* __restrict__ fd, BiState* __restrict__ st, SysMap sm, int S, int F) {
+static __global__ void k_bi_omega(const double* __restrict__ fd, BiState* __restrict__ st, SysMap sm, int S, int F) {
   int sy = blockIdx.x * blockDim.x + threadIdx.x;
   if (sy >= S || !st[sy].active) return;
   double d[4];
   sys_sums(fd, sy, sm, F, d);
   st[sy].omega = cdiv(make_double2(d[0], d[1]), make_double2(d[2], 0.0));
 }
-__global__ void k_bi_beta(const double* __restrict__ fd, BiState* __restrict__ st, int* __restrict__ upd, SysMap sm, int S, int F,
+static __global__ void k_bi_beta(const double* __restrict__ fd, BiState* __restrict__ st, int* __restrict__ upd, SysMap sm, int S, int F,
                           int itmax, int* __restrict__ any_active, int stop_true) {
   int sy = blockIdx.x * blockDim.x + threadIdx.x;
   if (sy >= S) return;
@@ -1047,7 +1201,7 @@ __global__ void __launch_bounds__(256) k_psi_resnorm(const cplx<T>* __restrict__
   }
   block_reduce_store<4>(acc, part + ((long long)blockIdx.y * ew.bpf + blockIdx.x) * 4, smm);
 }
-__global__ void k_psi_true_res(const double* __restrict__ fd, double* __restrict__ out, SysMap sm, int S, int F) {
+static __global__ void k_psi_true_res(const double* __restrict__ fd, double* __restrict__ out, SysMap sm, int S, int F) {
   int sy = blockIdx.x * blockDim.x + threadIdx.x;
   if (sy >= S) return;
   double d[4];
@@ -1096,7 +1250,7 @@ __global__ void __launch_bounds__(256) k_re_sumsq(const cplx<T>* __restrict__ w,
   block_reduce_store<1>(acc, part + ((long long)f * ew.bpf + blockIdx.x), smm);
 }
 // inv_s[f] = 1 / RMS (0 for a zero field)
-__global__ void k_inv_rms(const double* __restrict__ fd, double n, float* __restrict__ inv_s, int F) {
+static __global__ void k_inv_rms(const double* __restrict__ fd, double n, float* __restrict__ inv_s, int F) {
   int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= F) return;
   double ms = fd[f] / n;

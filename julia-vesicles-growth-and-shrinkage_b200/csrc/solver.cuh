@@ -99,22 +99,22 @@ struct Dims {
   double Lx, Ly, Lz;
 };
 
-__global__ void k_copy_mmax(const double* sch, double* mm, int R) {
+static __global__ void k_copy_mmax(const double* sch, double* mm, int R) {
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r < R) mm[r] = sch[r * 8 + 3];
   }
 
-__global__ void k_set_adt(const double* dt, double a, double* adt, int R) {
+static __global__ void k_set_adt(const double* dt, double a, double* adt, int R) {
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r < R) adt[r] = a / dt[r];
   }
 
-__global__ void k_area0(const double* asum, double cell, double* A0, int V) {
+static __global__ void k_area0(const double* asum, double cell, double* A0, int V) {
     int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v < V) A0[v] = asum[v] * cell;
   }
 
-__global__ void k_init_scalars(const double* sch, double* s, int R) {
+static __global__ void k_init_scalars(const double* sch, double* s, int R) {
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r < R) { s[r * 4 + 0] = 1.0; s[r * 4 + 1] = sch[r * 8 + 0]; s[r * 4 + 2] = sch[r * 8 + 1]; s[r * 4 + 3] = sch[r * 8 + 2]; }
   }
@@ -122,7 +122,7 @@ __global__ void k_init_scalars(const double* sch, double* s, int R) {
 // Condition of a Krylov WHILE node of a captured time step: 1 while any
 // system is active.  Bounded: after itmax + 1 evaluations the loop stops
 // whatever the flags say (and flags the overrun in *err, bit 3).
-__global__ void k_loop_cond(cudaGraphConditionalHandle hnd, const BiState* st_, int S, unsigned* trips, int limit,
+static __global__ void k_loop_cond(cudaGraphConditionalHandle hnd, const BiState* st_, int S, unsigned* trips, int limit,
                             int* err) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   int any = 0;
@@ -132,7 +132,7 @@ __global__ void k_loop_cond(cudaGraphConditionalHandle hnd, const BiState* st_, 
   cudaGraphSetConditional(hnd, any ? 1u : 0u);
 }
 
-__global__ void k_bi_flags(const BiState* st_, int* upd, int S) {
+static __global__ void k_bi_flags(const BiState* st_, int* upd, int S) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s < S) upd[s] = st_[s].active;
   }
@@ -545,6 +545,17 @@ class Solver : public SolverBase {
         if (!tma_var_ok(tma_var_comb)) tma_var_comb = v;
       }
     }
+    // VSAV_PSI_BULK overrides the choice of the bulk-copy-fed psi x pass (where eligible):
+    // 0 off, 1 on (the tuned block shape, else the first usable one), 2 + v block shape v
+    if (const char* env = getenv("VSAV_PSI_BULK")) {
+      const int b = atoi(env);
+      bulk_rows = b != 0 && bulk_eligible();
+      if (b >= 2) bulk_var = b - 2;
+      if (bulk_rows && !bulk_var_ok(bulk_var))
+        for (int v = BR_NV - 1; v >= 0; --v)
+          if (bulk_var_ok(v)) bulk_var = v;
+      if (!bulk_rows) bulk_var = 0;
+    }
     if constexpr (std::is_same<T, double>::value) {
       if (opt.psi_mixed && (nd == 2 || opt.psi3d_var)) {
         Options o2 = opt;
@@ -585,6 +596,16 @@ class Solver : public SolverBase {
   // ------------------------------------------------------------------ launch helpers
   EW ew(long long n) const {
     EW e; e.n = n; e.chunk = std::min<long long>(2048, n); e.bpf = (int)((n + e.chunk - 1) / e.chunk); return e;
+  }
+  // the Krylov vector passes of the psi solve (F fields of n slots): about eight
+  // 256-thread blocks per SM in all, each streaming a long contiguous range of one
+  // field (chunks of at least 2048 slots, a multiple of 1024), so the per-block
+  // reduction of the dot partials is amortised over many elements
+  EW ewv(long long n, int F) const {
+    const long long want = std::max<long long>(1, (148LL * 8 + F - 1) / std::max(F, 1));
+    long long chunk = (n + want - 1) / want;
+    chunk = std::max<long long>(2048, (chunk + 1023) / 1024 * 1024);
+    EW e; e.n = n; e.chunk = std::min<long long>(chunk, n); e.bpf = (int)((n + e.chunk - 1) / e.chunk); return e;
   }
   int gridfor(long long n, int bs = 256) const { long long b = (n + bs - 1) / bs; return (int)std::min<long long>(b, 148 * 16); }
   void fin(int K, int F, const EW& e, double* out) {
@@ -735,6 +756,7 @@ class Solver : public SolverBase {
   void rows_mul(C* t, long long nrows, bool full, int f0 = 0, int fc = 0) {
     const int rpf = g.Nz * g.Ny;                          // rows of one field
     if (fc == 0) fc = (int)(nrows / (2 * rpf));
+    if (full && bulk_rows && g.nd == 2 && nrows == 2LL * fc * g.Ny) { rows_mul_bulk(t, f0, fc); return; }
     int L = full ? g.Nx : g.Nx / 2, logL = ilog2(L);
     SysMap sm{dm.V, dm.R, d_run_of};
     int rowlen = full ? g.Nx : g.kp;
@@ -759,6 +781,65 @@ class Solver : public SolverBase {
       // reads + writes t1|t2 rows and reads M once per row
       prof.end(st, KC_ROWS_MUL, (double)nrows * ((full ? g.Nx : g.nkx) * 2.0 * sizeof(C) + g.Nx * sizeof(T)));
     })
+  }
+
+  // The bulk-copy-fed persistent form of the FULL x pass (k_rows_mul_bulk, FP32), in
+  // three block shapes (E, threads, ring slots); the autotuner times them against the
+  // classic kernel.  Row lengths 256 .. 2048 are compiled.
+  static constexpr int BR_NV = 3;
+  static constexpr int BR_E[BR_NV] = {16, 32, 32}, BR_NT[BR_NV] = {256, 128, 128}, BR_S[BR_NV] = {2, 2, 3};
+  int bulk_rows = 0;              // 1: the psi x pass runs as k_rows_mul_bulk (autotuned)
+  int bulk_var = 0;
+  int bulk_ctas[BR_NV] = {0, 0, 0};
+  bool bulk_var_ok(int v) const {
+    const int L = g.Nx, E = BR_E[v], NL = BR_NT[v] * E / L;
+    return v >= 0 && v < BR_NV && L >= 256 && L <= 2048 && L >= E * E && NL >= 1 && NL <= g.Ny;
+  }
+  bool bulk_eligible() const {
+    if constexpr (!std::is_same<T, float>::value) return false;
+    else {
+      if (g.nd != 2 || !psi_full() || vt12 == nullptr) return false;
+      for (int v = 0; v < BR_NV; ++v)
+        if (bulk_var_ok(v)) return true;
+      return false;
+    }
+  }
+  template <int E_, int NT_, int S_, int LOGL>
+  void launch_rows_bulk(C* t, int f0, int fc, int var) {
+    if constexpr (std::is_same<T, float>::value) {
+      using G = BulkRows<E_, NT_, LOGL, S_>;
+      SysMap sm{dm.V, dm.R, d_run_of};
+      const long long ntiles = 2LL * fc * (g.Ny / G::NL);
+      const int grid = (int)std::min<long long>(ntiles, tma_grid((const void*)k_rows_mul_bulk<E_, NT_, LOGL, S_>, NT_,
+                                                                  G::smem, bulk_ctas[var]));
+      prof.begin(st);
+      k_rows_mul_bulk<E_, NT_, LOGL, S_><<<grid, NT_, G::smem, st>>>(t, Mpsi, (float)(1.0 / g.P), g.Ny, fc, f0, ntiles, sm,
+                                                                     bupd, tab, d_err);
+      VSAV_COUNT_LAUNCH();
+      VSAV_LAUNCH_CHECK();
+      prof.end(st, KC_ROWS_MUL, (double)2 * fc * g.Ny * (g.Nx * 2.0 * sizeof(C) + g.Nx * sizeof(T)));
+    }
+  }
+  template <int LOGL>
+  void rows_bulk_L(C* t, int f0, int fc, int var) {
+    if constexpr (BulkRows<BR_E[0], BR_NT[0], LOGL, BR_S[0]>::ok)
+      if (var == 0) { launch_rows_bulk<BR_E[0], BR_NT[0], BR_S[0], LOGL>(t, f0, fc, 0); return; }
+    if constexpr (BulkRows<BR_E[1], BR_NT[1], LOGL, BR_S[1]>::ok)
+      if (var == 1) { launch_rows_bulk<BR_E[1], BR_NT[1], BR_S[1], LOGL>(t, f0, fc, 1); return; }
+    if constexpr (BulkRows<BR_E[2], BR_NT[2], LOGL, BR_S[2]>::ok)
+      if (var == 2) { launch_rows_bulk<BR_E[2], BR_NT[2], BR_S[2], LOGL>(t, f0, fc, 2); return; }
+    throw std::runtime_error("bulk x pass: block shape not compiled for this row length");
+  }
+  void rows_mul_bulk(C* t, int f0, int fc, int var = -1) {
+    if (var < 0) var = bulk_var;
+    if (!bulk_var_ok(var)) throw std::runtime_error("bulk x pass: block shape unusable at this size");
+    switch (ilog2(g.Nx)) {
+      case 8: rows_bulk_L<8>(t, f0, fc, var); break;
+      case 9: rows_bulk_L<9>(t, f0, fc, var); break;
+      case 10: rows_bulk_L<10>(t, f0, fc, var); break;
+      case 11: rows_bulk_L<11>(t, f0, fc, var); break;
+      default: throw std::runtime_error("bulk x pass: unsupported row length");
+    }
   }
 
   // fused FULL-form operator column passes (fields f0 .. f0+fc-1; t1/t2 chunk-local)
@@ -1084,7 +1165,7 @@ class Solver : public SolverBase {
     std::lock_guard<std::mutex> lk(tune_mutex());
     std::vector<int> c(choice, choice + FAM_N);
     c.push_back(split_comb);
-    c.push_back(tma_cols | tma_var_inv2 << 1 | tma_var_comb << 3);
+    c.push_back(tma_cols | tma_var_inv2 << 1 | tma_var_comb << 3 | bulk_rows << 5 | bulk_var << 6);
     tune_cache()[tune_key()] = c;
     if (tfile && *tfile) {
       std::map<std::string, std::vector<int>> fm;
@@ -1098,6 +1179,9 @@ class Solver : public SolverBase {
     tma_var_comb = (code >> 3) & 3;
     if (tma_var_inv2 >= TMA_NV || tma_var_comb >= TMA_NV) tma_var_inv2 = tma_var_comb = 0;
     tma_cols = (code & 1) && tma_eligible() && tma_var_ok(tma_var_inv2) && tma_var_ok(tma_var_comb);
+    bulk_var = (code >> 6) & 3;
+    bulk_rows = ((code >> 5) & 1) && bulk_eligible() && bulk_var_ok(bulk_var);
+    if (!bulk_rows) bulk_var = 0;
   }
   // the variants in use, as JSON: {"key", "source", "split", families: "E<e>/NT<nt>"}
   std::string tuning_json() const {
@@ -1106,6 +1190,10 @@ class Solver : public SolverBase {
     std::string o = "{\"key\": \"" + tune_key() + "\", \"source\": \"" + tune_source + "\", \"psi_forward_combine\": \"" +
                     (split_comb ? "split" : "fused") + "\", \"psi_column_passes\": \"" +
                     (tma_cols ? "tma" : "classic") + "\", \"variants\": {";
+    o += std::string("\"psi_rows\": \"") +
+         (bulk_rows ? "bulk E" + std::to_string(BR_E[bulk_var]) + "/NT" + std::to_string(BR_NT[bulk_var]) + "/S" +
+                          std::to_string(BR_S[bulk_var])
+                    : std::string("classic")) + "\", ";
     if (tma_cols)
       o += "\"psi_inv2_tma\": \"E" + std::to_string(TMA_VE[tma_var_inv2]) + "/NT" + std::to_string(TMA_VNT[tma_var_inv2]) +
            "\", \"psi_comb_tma\": \"E" + std::to_string(TMA_VE[tma_var_comb]) + "/NT" +
@@ -1214,6 +1302,28 @@ class Solver : public SolverBase {
                              (split_comb ? split_ms : tune_ms[FAM_PSI_COMB][choice[FAM_PSI_COMB]]);
       tma_cols = tma_ms < classic;
     }
+    // the bulk-copy-fed x pass against the classic one (as chosen above)
+    bulk_rows = 0;
+    bulk_var = 0;
+    if (bulk_eligible()) {
+      const int Fc = psi_chunk();                        // the classic pass was timed on one chunk too
+      double best = 1e30;
+      int bv = -1;
+      for (int v = 0; v < BR_NV; ++v) {
+        if (!bulk_var_ok(v)) continue;
+        auto fn = [&]() { rows_mul_bulk(vt12, 0, Fc, v); };
+        fn();
+        VSAV_CUDA(cudaEventRecord(e0, st));
+        for (int k = 0; k < 3; ++k) fn();
+        VSAV_CUDA(cudaEventRecord(e1, st));
+        VSAV_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        VSAV_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        bulk_ms[v] = ms / 3;
+        if (bulk_ms[v] < best) { best = bulk_ms[v]; bv = v; }
+      }
+      if (bv >= 0 && best < tune_ms[FAM_MUL][choice[FAM_MUL]]) { bulk_rows = 1; bulk_var = bv; }
+    }
     prof.on = was;
     if (getenv("VSAV_VERBOSE")) {
       const char* nm[FAM_N] = {"rows_r2c", "rows_c2r", "rows_c2c", "rows_mul", "cols", "cols_psi", "psi_inv2", "psi_comb",
@@ -1227,6 +1337,8 @@ class Solver : public SolverBase {
       fprintf(stderr, "[vsav autotune %s] forward pass + combine: %s (split %.3f ms); TMA column passes: %s (%.3f ms)\n",
               std::is_same<T, double>::value ? "fp64" : "fp32", split_comb ? "split" : "fused", split_ms,
               tma_cols ? "on" : "off", tma_ms);
+      fprintf(stderr, "[vsav autotune %s] bulk x pass: %s (%.3f / %.3f / %.3f ms)\n",
+              std::is_same<T, double>::value ? "fp64" : "fp32", bulk_rows ? "on" : "off", bulk_ms[0], bulk_ms[1], bulk_ms[2]);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -1664,7 +1776,7 @@ class Solver : public SolverBase {
   // y = P^-1 A in (+ dots), chunk by chunk: y-inverse (2 multipliers), fused
   // x pass (inverse, x M_psi, forward), y-forward, combine
   EW dot_ew{};                 // partial layout of the dots of the last matvec
-  double split_ms = 0.0, tma_ms = 0.0;
+  double split_ms = 0.0, tma_ms = 0.0, bulk_ms[3] = {0.0, 0.0, 0.0};
   bool use_split() const { return split_comb != 0; }
   bool fused_ops = true;       // FULL form: fused column passes (VSAV_PSI_FUSED=0: separate kernels)
   void matvec(const C* in, C* out, int mode, const C* svec, bool precond = true) {
@@ -1780,7 +1892,7 @@ class Solver : public SolverBase {
   void psi_check_residual(const C* x) {
     const int V = dm.V, R = dm.R, S = 3 * R;
     const long long F = 3LL * V, n = psi_n();
-    EW e = ew(n);
+    EW e = ewv(n, (int)F);
     SysMap sm{V, R, d_run_of};
     VSAV_CUDA(cudaMemsetAsync(bupd, 0xff, S * sizeof(int), st));     // every system active in A x
     matvec(x, vt, 0, nullptr, false);
@@ -1870,7 +1982,7 @@ class Solver : public SolverBase {
     const int V = dm.V, R = dm.R, S = 3 * R;
     const long long F = 3LL * V, n = psi_n();
     const bool full = psi_full();
-    EW e = ew(n);
+    EW e = ewv(n, (int)F);
     VGeom vg = vgeom();
     SysMap sm{V, R, d_run_of};
     k_psi_init<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(vb, x, vr, vp, d_adt, mmax_r, ph.S4, vg, sm, e, part); VSAV_COUNT_LAUNCH();
@@ -1919,7 +2031,7 @@ class Solver : public SolverBase {
   void psi_flex(C* x, double rtol, int itmax) {
     const int V = dm.V, R = dm.R, S = 3 * R;
     const long long F = 3LL * V, n = psi_n();
-    EW e = ew(n);
+    EW e = ewv(n, (int)F);
     VGeom vg = vgeom();
     SysMap sm{V, R, d_run_of};
     if (opt.psi_precond == 2 && !net_ok)
@@ -1962,7 +2074,7 @@ class Solver : public SolverBase {
   // y = Re IFFT(D^-1 in) per field, s its RMS, M~ = (M_psi - 0.075) / 0.025.
   void precond_apply(const C* in, C* out) {
     const long long F = 3LL * dm.V, n = psi_n();
-    EW e = ew(n);
+    EW e = ewv(n, (int)F);
     SysMap sm{dm.V, dm.R, d_run_of};
     k_psi_diag<T><<<dim3(e.bpf, (unsigned)F), 256, 0, st>>>(in, out, d_adt, mmax_r, ph.S4, vgeom(), sm, e); VSAV_COUNT_LAUNCH();
     VSAV_LAUNCH_CHECK();
@@ -2294,5 +2406,12 @@ void Solver<T>::psi_solve_mixed() {
     psi_finish();
   }
 }
+
+// The two instantiations are compiled in their own translation units
+// (solver_f32.cu, solver_f64.cu); the C ABI creates them through these.
+SolverBase* make_solver_f32(const Dims& d, const Phys& p, const Options& o, const int* run_sizes, const double* psi_in,
+                            const double* psi_out);
+SolverBase* make_solver_f64(const Dims& d, const Phys& p, const Options& o, const int* run_sizes, const double* psi_in,
+                            const double* psi_out);
 
 }  // namespace vsav

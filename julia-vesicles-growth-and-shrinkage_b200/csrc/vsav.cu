@@ -143,9 +143,9 @@ int vsav_create(const vsav_config* cfg, const vsav_options* opt, vsav_handle** o
       if (cfg->Nx > CH) throw std::runtime_error("Nx too large for the full-spectrum psi form");
     }
     if (o.precision == VSAV_FP32)
-      h->s = new Solver<float>(d, p, so, rs.data(), cfg->psi_in_v, cfg->psi_out_v);
+      h->s = make_solver_f32(d, p, so, rs.data(), cfg->psi_in_v, cfg->psi_out_v);
     else
-      h->s = new Solver<double>(d, p, so, rs.data(), cfg->psi_in_v, cfg->psi_out_v);
+      h->s = make_solver_f64(d, p, so, rs.data(), cfg->psi_in_v, cfg->psi_out_v);
     h->R = o.n_runs; h->V = V; h->nd = cfg->ndim;
     std::vector<double> dt(o.n_runs, cfg->dt);
     h->s->set_dt(dt.data());

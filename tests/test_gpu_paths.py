@@ -3,7 +3,9 @@ default path's results: the unfused psi operator (VSAV_PSI_FUSED=0), the psi
 operator in L2-sized chunks of fields (VSAV_PSI_CHUNK_MB), eager launches
 instead of CUDA-graph replay (VSAV_GRAPH=0), and either form of the operator's
 forward pass (VSAV_PSI_SPLIT=1: k_psi_cols_fwd2 + k_psi_combz; 0: the fused
-k_psi_cols_comb), whichever the autotuner picked."""
+k_psi_cols_comb), whichever the autotuner picked, and the operator's x pass as
+the classic kernel (VSAV_PSI_BULK=0) or as each block shape of the bulk-copy-fed
+persistent kernel (VSAV_PSI_BULK=2, 3, 4; FP32 psi solves only)."""
 import numpy as np
 import pytest
 
@@ -28,7 +30,8 @@ def run(kw, phi, psi, prec, steps=3):
 
 @pytest.mark.parametrize("prec", ["fp64", "mixed", "fp32"])
 @pytest.mark.parametrize("env", [("VSAV_PSI_FUSED", "0"), ("VSAV_PSI_CHUNK_MB", "1"), ("VSAV_GRAPH", "0"),
-                                 ("VSAV_PSI_SPLIT", "1"), ("VSAV_PSI_SPLIT", "0")])
+                                 ("VSAV_PSI_SPLIT", "1"), ("VSAV_PSI_SPLIT", "0"), ("VSAV_PSI_BULK", "0"),
+                                 ("VSAV_PSI_BULK", "2"), ("VSAV_PSI_BULK", "3"), ("VSAV_PSI_BULK", "4")])
 def test_switches_keep_the_results(prec, env, monkeypatch):
     from vsav import ics
     kw, phi, psi, _ = ics.workload("multi2d_512x4", seed=2, n_override=256, N_override=2, eps_override=0.08)
@@ -47,3 +50,21 @@ def test_switches_keep_the_results(prec, env, monkeypatch):
     np.testing.assert_allclose(alt["E"], base["E"], rtol=1e-6 if prec == "fp32" else 1e-10)
     if prec != "fp32":
         assert np.array_equal(alt["iters"], base["iters"])
+
+
+@pytest.mark.parametrize("n", [512, 1024, 2048])
+@pytest.mark.parametrize("shape", ["2", "3", "4"])
+def test_bulk_x_pass_block_shapes(n, shape, monkeypatch):
+    """Every block shape of the bulk-copy-fed x pass at the row lengths 512, 1024
+    and 2048 (E 32 is usable from 1024 on) gives the classic kernel's results in
+    the mixed path, whose FP32 psi solves run through it."""
+    from vsav import ics
+    kw, phi, psi, _ = ics.workload("multi2d_512x4", seed=3, n_override=n, N_override=1, eps_override=0.08)
+    kw["dt"] = 1e-6
+    monkeypatch.setenv("VSAV_PSI_BULK", "0")
+    base = run(kw, phi, psi, "mixed", steps=2)
+    monkeypatch.setenv("VSAV_PSI_BULK", shape)
+    alt = run(kw, phi, psi, "mixed", steps=2)
+    for k in FIELDS:
+        assert rel(alt[k], base[k]) < 1e-10, (k, rel(alt[k], base[k]))
+    np.testing.assert_allclose(alt["E"], base["E"], rtol=1e-10)
