@@ -425,7 +425,8 @@ def run_ours(args):
         px = 3 * V * kw["Nx"] * kw["Ny"]
         tf = pn["launches"] * px * NET_FLOP_PER_PIXEL / (pn["ms"] / 1000.0) / 1e12
         tot = max(sum(p["ms"] for p in prof.values()), 1e-9)
-        return {"bound": "tensor", "kernel": "k_net_apply (mma.sync bf16)", "arm": arm, "achieved": tf,
+        kern = "k_net_apply_tc (tcgen05 bf16)" if os.environ.get("VSAV_NET_TC", "0") != "0" else "k_net_apply (mma.sync bf16)"
+        return {"bound": "tensor", "kernel": kern, "arm": arm, "achieved": tf,
                 "peak": tflops_peak, "unit": "TFLOP/s", "frac": tf / tflops_peak, "peak_kind": "measured bf16 burst",
                 "ms_per_launch": pn["ms"] / pn["launches"], "launches_per_step": pn["launches"] / nsteps,
                 "share_of_profiled_time": pn["ms"] / tot, "flop_per_pixel": NET_FLOP_PER_PIXEL}

@@ -4,6 +4,7 @@
 #include "../../include/vsav.h"
 #include "net.cuh"
 #include "net_apply.cuh"
+#include "net_tc.cuh"
 
 #include <string>
 
@@ -15,6 +16,8 @@ struct vsav_net {
   std::string err;
   uint32_t* frag = nullptr;        // packed mma fragments of the BF16 weights
   float* fbias = nullptr;
+  uint4* timg = nullptr;           // B operands of the tcgen05 kernel (net_pack_tc image)
+  int* derr = nullptr;             // error word of the tcgen05 kernel's bounded waits
   float* tbuf = nullptr;           // gathered targets of a training batch
   bool frags_dirty = true;
 };
@@ -44,8 +47,11 @@ void refresh_frags(vsav_net* h) {
   std::vector<uint32_t> fr(NF_WORDS);
   std::vector<float> bias(NF_BIAS, 0.f);
   net_pack(wb.data(), fr.data(), bias.data());
+  std::vector<uint16_t> img(NT_WBYTES / 2);
+  net_pack_tc(wb.data(), img.data());
   VSAV_CUDA(cudaMemcpyAsync(h->frag, fr.data(), NF_WORDS * 4, cudaMemcpyHostToDevice, h->n.st));
   VSAV_CUDA(cudaMemcpyAsync(h->fbias, bias.data(), NF_BIAS * 4, cudaMemcpyHostToDevice, h->n.st));
+  VSAV_CUDA(cudaMemcpyAsync(h->timg, img.data(), NT_WBYTES, cudaMemcpyHostToDevice, h->n.st));
   VSAV_CUDA(cudaStreamSynchronize(h->n.st));
   h->frags_dirty = false;
 }
@@ -91,6 +97,8 @@ int vsav_net_create(int64_t cap_pixels, int32_t device, vsav_net** out) {
     h->n.init(cap_pixels, (int)std::min<long long>(cap_pixels / 121, 1 << 20));
     h->frag = h->n.alloc<uint32_t>(NF_WORDS);
     h->fbias = h->n.alloc<float>(NF_BIAS);
+    h->timg = h->n.alloc<uint4>(NT_WBYTES / 16);
+    h->derr = h->n.alloc<int>(1);
     h->tbuf = h->n.alloc<float>((size_t)cap_pixels);
   } catch (const std::exception& ex) {
     g_net_create_error = ex.what();
@@ -132,22 +140,37 @@ int vsav_net_forward(vsav_net* h, const float* x, int32_t B, int32_t H, int32_t 
     const bool P = periodic != 0;
     n.check(B, H, W, P);
     const int Ho = P ? H : H - 10, Wo = P ? W : W - 10;
-    if (impl == 1) {
+    if (impl == 1 || impl == 2) {
       if (!P) throw std::runtime_error("the fused kernel is periodic only");
       if (H % NA_T || W % NA_T || (H & (H - 1)) || (W & (W - 1)))
         throw std::runtime_error("the fused kernel needs H and W powers of two, multiples of 32");
       refresh_frags(h);
       VSAV_CUDA(cudaMemcpyAsync(n.act[0], x, (size_t)B * 2 * H * W * 4, cudaMemcpyDefault, n.st));
-      VSAV_CUDA(cudaFuncSetAttribute(k_net_apply<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, NA_SMEM));
-      dim3 grid((H / NA_T) * (W / NA_T), B);
-      k_net_apply<0><<<grid, NA_THREADS, NA_SMEM, n.st>>>(n.act[0], nullptr, nullptr, n.act[NET_NL], H, W, 1, h->frag,
-                                                          h->fbias); VSAV_COUNT_LAUNCH();
-      VSAV_LAUNCH_CHECK();
+      if (impl == 1) {
+        VSAV_CUDA(cudaFuncSetAttribute(k_net_apply<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, NA_SMEM));
+        dim3 grid((H / NA_T) * (W / NA_T), B);
+        k_net_apply<0><<<grid, NA_THREADS, NA_SMEM, n.st>>>(n.act[0], nullptr, nullptr, n.act[NET_NL], H, W, 1, h->frag,
+                                                            h->fbias); VSAV_COUNT_LAUNCH();
+        VSAV_LAUNCH_CHECK();
+      } else {
+        VSAV_CUDA(net_tc_attributes<0>());
+        int nsm = 0;
+        VSAV_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
+        const long long tiles = (long long)B * (H / NT_T) * (W / NT_T);
+        VSAV_CUDA(cudaMemsetAsync(h->derr, 0, sizeof(int), n.st));
+        k_net_apply_tc<0><<<(unsigned)std::min<long long>(tiles, nsm), NT_THREADS, NT_SMEM, n.st>>>(
+            n.act[0], nullptr, nullptr, n.act[NET_NL], H, W, 1, B, h->timg, h->fbias, h->derr); VSAV_COUNT_LAUNCH();
+        VSAV_LAUNCH_CHECK();
+        int e = 0;
+        VSAV_CUDA(cudaMemcpyAsync(&e, h->derr, sizeof(int), cudaMemcpyDeviceToHost, n.st));
+        VSAV_CUDA(cudaStreamSynchronize(n.st));
+        if (e) throw std::runtime_error("CUDA: device-side bound exceeded in the tcgen05 network kernel");
+      }
     } else if (impl == 0) {
       VSAV_CUDA(cudaMemcpyAsync(n.act[0], x, (size_t)B * 2 * H * W * 4, cudaMemcpyDefault, n.st));
       if (P) n.forward<true>(B, H, W); else n.forward<false>(B, H, W);
     } else {
-      throw std::runtime_error("impl must be 0 (FP32 per layer) or 1 (fused tensor cores)");
+      throw std::runtime_error("impl must be 0 (FP32 per layer), 1 (fused, mma.sync) or 2 (fused, tcgen05)");
     }
     VSAV_CUDA(cudaMemcpyAsync(out, n.act[NET_NL], (size_t)B * Ho * Wo * 4, cudaMemcpyDefault, n.st));
     VSAV_CUDA(cudaStreamSynchronize(n.st));

@@ -18,6 +18,7 @@
 #include <mutex>
 #include "psi.cuh"
 #include "net_apply.cuh"
+#include "net_tc.cuh"
 
 namespace vsav {
 
@@ -85,8 +86,9 @@ class SolverBase {
   virtual void profile(int enable) = 0;
   virtual void profile_read(int cls, double* out3) = 0;
   virtual cudaStream_t stream() = 0;
-  // learned psi preconditioner: packed mma fragments + biases (net_pack)
-  virtual void set_psi_net(const uint32_t* frags, const float* bias) = 0;
+  // learned psi preconditioner: packed mma fragments + biases (net_pack) and
+  // the tcgen05 kernel's B-operand image (net_pack_tc)
+  virtual void set_psi_net(const uint32_t* frags, const float* bias, const uint16_t* timg) = 0;
   // snapshots of the psi BiCGSTAB iterates (training data of the network)
   virtual void harvest(int cap) = 0;
   virtual long long harvest_read(float* out, long long cap, int* nsnap) = 0;
@@ -404,6 +406,9 @@ class Solver : public SolverBase {
   uint32_t* nfrag = nullptr;                 // learned preconditioner weights (mma fragments)
   float *nbias = nullptr, *inv_s = nullptr;
   bool net_ok = false;
+  uint4* ntimg = nullptr;                    // the same weights as tcgen05 B operands
+  int net_sms = 1;                           // SMs of the device: the persistent tcgen05 grid
+  int net_impl = 1;                          // network kernel: 1 k_net_apply (mma.sync), 2 k_net_apply_tc (tcgen05)
   float* hv = nullptr;                       // harvested iterates
   int hv_cap = 0, hv_count = 0;
   BiState* bst = nullptr; int *bupd = nullptr, *d_any = nullptr;
@@ -525,7 +530,16 @@ class Solver : public SolverBase {
         if (!psi_full()) throw std::runtime_error("the learned psi preconditioner needs the full-spectrum psi form");
         if (g.Nx < NA_T || g.Ny < NA_T) throw std::runtime_error("the learned psi preconditioner needs Nx, Ny >= 32");
         nfrag = dalloc<uint32_t>(NF_WORDS); nbias = dalloc<float>(NF_BIAS); inv_s = dalloc<float>(3 * V);
+        ntimg = dalloc<uint4>(NT_WBYTES / 16);
         VSAV_CUDA(cudaFuncSetAttribute(k_net_apply<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, NA_SMEM));
+        VSAV_CUDA(net_tc_attributes<1>());
+        // VSAV_NET_TC=1 selects the tcgen05 kernel (read once, for this handle's life); the
+        // mma.sync kernel is the default: at 16 channels a tcgen05.mma (M 128, N 16, K 16)
+        // is issue-bound, so the warp-level MMAs of eight warps finish the layer sooner
+        if (const char* env = getenv("VSAV_NET_TC")) net_impl = atoi(env) != 0 ? 2 : 1;
+        int dev = 0;
+        VSAV_CUDA(cudaGetDevice(&dev));
+        VSAV_CUDA(cudaDeviceGetAttribute(&net_sms, cudaDevAttrMultiProcessorCount, dev));
       }
     }
     long long nh = std::max<long long>(3LL * V, 2LL * R * nd) * std::max<long long>(g.P, (long long)g.Nz * g.Ny * g.nkx * 2);
@@ -1202,6 +1216,7 @@ class Solver : public SolverBase {
       o += std::string(f ? ", " : "") + "\"" + nm[f] + "\": \"E" + std::to_string(vE(choice[f])) + "/NT" +
            std::to_string(VNT[choice[f]]) + "\"";
     o += "}";
+    if (ntimg) o += std::string(", \"psi_net_kernel\": \"") + (net_impl == 2 ? "k_net_apply_tc (tcgen05)" : "k_net_apply (mma.sync)") + "\"";
     if (psi32) o += ", \"psi_fp32\": " + psi32->tuning_json();
     return o + "}";
   }
@@ -2088,8 +2103,14 @@ class Solver : public SolverBase {
       fin(1, (int)F, e, fd2);
       k_inv_rms<<<(unsigned)((F + 127) / 128), 128, 0, st>>>(fd2, (double)n, inv_s, (int)F); VSAV_COUNT_LAUNCH();
       prof.begin(st);
-      k_net_apply<1><<<dim3((unsigned)((g.Ny / NA_T) * (g.Nx / NA_T)), (unsigned)F), NA_THREADS, NA_SMEM, st>>>(
-          w1, Mpsi, inv_s, w2, g.Ny, g.Nx, dm.V, nfrag, nbias); VSAV_COUNT_LAUNCH();
+      if (net_impl == 2) {
+        const long long tiles = F * (g.Ny / NT_T) * (g.Nx / NT_T);
+        k_net_apply_tc<1><<<(unsigned)std::min<long long>(tiles, net_sms), NT_THREADS, NT_SMEM, st>>>(
+            w1, Mpsi, inv_s, w2, g.Ny, g.Nx, dm.V, (int)F, ntimg, nbias, d_err); VSAV_COUNT_LAUNCH();
+      } else {
+        k_net_apply<1><<<dim3((unsigned)((g.Ny / NA_T) * (g.Nx / NA_T)), (unsigned)F), NA_THREADS, NA_SMEM, st>>>(
+            w1, Mpsi, inv_s, w2, g.Ny, g.Nx, dm.V, nfrag, nbias); VSAV_COUNT_LAUNCH();
+      }
       VSAV_LAUNCH_CHECK();
       prof.end(st, KC_NET, (double)F * n * (2.0 * sizeof(C)) + (double)dm.V * g.P * sizeof(T));
       rows_c2c<false>(w2, nullptr, w2, 1.0, F * g.Ny);
@@ -2097,11 +2118,12 @@ class Solver : public SolverBase {
     }
   }
 
-  void set_psi_net(const uint32_t* frags, const float* bias) override {
-    if (psi32) { psi32->set_psi_net(frags, bias); return; }
+  void set_psi_net(const uint32_t* frags, const float* bias, const uint16_t* timg) override {
+    if (psi32) { psi32->set_psi_net(frags, bias, timg); return; }
     if (!nfrag) throw std::runtime_error("the handle was not created with the learned psi preconditioner (psi_precond = 2)");
     VSAV_CUDA(cudaMemcpyAsync(nfrag, frags, NF_WORDS * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
     VSAV_CUDA(cudaMemcpyAsync(nbias, bias, NF_BIAS * sizeof(float), cudaMemcpyHostToDevice, st));
+    VSAV_CUDA(cudaMemcpyAsync(ntimg, timg, NT_WBYTES, cudaMemcpyHostToDevice, st));
     VSAV_CUDA(cudaStreamSynchronize(st));
     net_ok = true;
   }

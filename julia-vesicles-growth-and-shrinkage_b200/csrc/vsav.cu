@@ -386,7 +386,9 @@ int vsav_set_psi_net(vsav_handle* h, const double* theta) {
     std::vector<uint32_t> fr(NF_WORDS);
     std::vector<float> bias(NF_BIAS, 0.f);
     net_pack(wb.data(), fr.data(), bias.data());
-    h->s->set_psi_net(fr.data(), bias.data());
+    std::vector<uint16_t> img(NT_WBYTES / 2);
+    net_pack_tc(wb.data(), img.data());
+    h->s->set_psi_net(fr.data(), bias.data(), img.data());
     return VSAV_OK;
   });
 }

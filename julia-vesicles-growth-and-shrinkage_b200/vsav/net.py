@@ -76,13 +76,16 @@ class Net:
         self._chk(self.lib.vsav_net_get_params(self.h, L.dptr(th), int(rounded)))
         return th
 
-    def forward(self, x: np.ndarray, periodic: bool = True, fused: bool = False) -> np.ndarray:
+    def forward(self, x: np.ndarray, periodic: bool = True, fused: bool = False, impl: int = None) -> np.ndarray:
+        """Network output; impl 0: FP32 per-layer kernels, 1 (fused=True): the
+        fused mma.sync kernel, 2: the fused tcgen05 kernel."""
+        impl = (1 if fused else 0) if impl is None else int(impl)
         x = np.ascontiguousarray(x, dtype=np.float32)
         B, C, H, W = x.shape
         assert C == 2
         Ho, Wo = (H, W) if periodic else (H - 10, W - 10)
         out = np.empty((B, 1, Ho, Wo), np.float32)
-        self._chk(self.lib.vsav_net_forward(self.h, _fptr(x), B, H, W, int(periodic), int(fused), _fptr(out)))
+        self._chk(self.lib.vsav_net_forward(self.h, _fptr(x), B, H, W, int(periodic), impl, _fptr(out)))
         return out
 
     def grad(self, x: np.ndarray, t: np.ndarray, periodic: bool, residual_c0=None):

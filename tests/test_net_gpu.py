@@ -90,6 +90,31 @@ def test_fused_tensor_core_inference():
     n.close()
 
 
+@pytest.mark.parametrize("B,H,W", [(3, 64, 64), (1, 32, 32), (2, 32, 128), (5, 128, 64)])
+def test_tcgen05_inference(B, H, W):
+    """The fused tcgen05 kernel (implicit GEMM on the fifth-generation tensor
+    cores, accumulators in tensor memory) computes the network of the FP64
+    oracle with BF16 activations, like the mma.sync kernel: the same error
+    bound against the oracle, and close to the mma.sync kernel (the two differ
+    only in the FP32 summation order, through BF16 roundings of activations)."""
+    from oracle import precond_net as P
+    from vsav.net import Net
+    rng = np.random.default_rng(11 + B + H)
+    th = _theta(5)
+    x = rng.standard_normal((B, 2, H, W)).astype(np.float32)
+    n = Net(B * H * W)
+    n.set_params(th)
+    ref = P.forward(th.astype(np.float32).astype(np.float64), x.astype(np.float64), True)
+    out_mma = n.forward(x, periodic=True, impl=1)
+    out_tc = n.forward(x, periodic=True, impl=2)
+    assert rel(out_tc, ref) < 2e-2, rel(out_tc, ref)
+    assert rel(out_tc, out_mma) < 2e-2, rel(out_tc, out_mma)
+    # every output pixel is written: no tile or M-tile is skipped
+    assert np.isfinite(out_tc).all()
+    assert np.array_equal(n.forward(x, periodic=True, impl=2), out_tc)
+    n.close()
+
+
 def test_training_reduces_loss():
     """Adam on the GPU kernels fits a teacher network of the same shape."""
     import torch
@@ -138,10 +163,13 @@ def test_flexible_diag_matches_reference_solve():
     assert np.all(out["flex_diag_it"] > 0)
 
 
+@pytest.mark.parametrize("net_tc", ["1", "0"])
 @pytest.mark.parametrize("prec", ["fp32", "mixed"])
-def test_learned_preconditioner_solves_to_tolerance(prec):
+def test_learned_preconditioner_solves_to_tolerance(prec, net_tc, monkeypatch):
     """Any network (here an untrained one) only changes the Krylov path: the
-    flexible solve still reaches the same solution."""
+    flexible solve still reaches the same solution, with the network on the
+    mma.sync kernel (the default) or the tcgen05 kernel (VSAV_NET_TC=1)."""
+    monkeypatch.setenv("VSAV_NET_TC", net_tc)
     kw, g = load_golden("multi2d_n64_N2")
     ref = _handle(kw, precision="fp64")
     ref.init_state(g["phi0"], g["psi0"])
