@@ -71,9 +71,9 @@ class Cfg:
         self.Lz = kw.get("Lz", 0.0)
 
 
-def workload(seed):
+def workload(seed, n_vesicles=None):
     from vsav import ics
-    kw, phi, psi, _ = ics.workload(WORKLOAD, seed=seed)
+    kw, phi, psi, _ = ics.workload(WORKLOAD, seed=seed, N_override=n_vesicles)
     kw["dt"] = DT
     return kw, phi, psi
 
@@ -338,7 +338,7 @@ def run_ours(args):
         tflops_peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"])
     except Exception:
         tflops_peak = 1590.0
-    kw, phi, psi = workload(rank)
+    kw, phi, psi = workload(rank, args.vesicles)
     V = kw["N"]
     head = args.arm
     K, W = args.steps, args.warmup
@@ -361,7 +361,7 @@ def run_ours(args):
     if args.quick:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": K,
-                              "warmup": W, "ms_per_step": ms_max / K, "quick": True, "arm": head,
+                              "warmup": W, "ms_per_step": ms_max / K, "quick": True, "arm": head, "vesicles": V,
                               "gpu_launches": int(launches), "clocks": clocks, "psi_iters_last_step": iters,
                               "tuning": h.tuning()}), flush=True)
         h.close()
@@ -642,11 +642,15 @@ def main():
     ap.add_argument("--arm", default="mixed_krylov_diag", choices=list(ARMS),
                     help="the configuration of the headline value")
     ap.add_argument("--arms", default="", help="comma-separated subset of the compared configurations")
+    ap.add_argument("--vesicles", type=int, default=None,
+                    help="with --quick: fewer vesicles on the 1024^2 grid (smaller profiler captures)")
     ap.add_argument("--workload", default="multi2d_1024x8",
                     choices=["multi2d_1024x8", "ensemble_256x64", "multi2d_512x4", "single3d_128",
                              "single3d_128_psivar"],
                     help="anything but multi2d_1024x8 prints its own comparison line, not the headline")
     args = ap.parse_args()
+    if args.vesicles is not None and not args.quick:
+        ap.error("--vesicles changes the workload: --quick runs only")
     if args.workload == "ensemble_256x64":
         run_ensemble(args)
         return
