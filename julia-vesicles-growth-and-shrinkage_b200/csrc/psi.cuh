@@ -1009,7 +1009,11 @@ __global__ void __launch_bounds__(256, 2) k_psi_update(cplx<T>* __restrict__ x, 
                                                     const cplx<T>* __restrict__ shat, const double* __restrict__ adt_r,
                                                     const double* __restrict__ mmax_r, double S4) {
   __shared__ double smm[2 * 4 * 8];
-  KSum acc[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+  // per-thread sums: compensated in the FP64 solve (parity path); plain FP64 in the
+  // FP32 solve, whose terms are products of FP32 values (a thread sums ~100 of them,
+  // ~1e-14 relative), compensated across threads and blocks either way
+  using Acc = typename std::conditional<std::is_same<T, float>::value, PlainSum, KSum>::type;
+  Acc acc[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
   const int f = blockIdx.y;
   const BiState& b = st[sm.sys(f)];
   if (b.active) {
@@ -1064,7 +1068,10 @@ __global__ void __launch_bounds__(256, 2) k_psi_update(cplx<T>* __restrict__ x, 
       }
     }
   }
-  block_reduce_store<4>(acc, part + ((long long)blockIdx.y * ew.bpf + blockIdx.x) * 4, smm);
+  KSum ks[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) ks[k] = {acc[k].s, acc[k].c};
+  block_reduce_store<4>(ks, part + ((long long)blockIdx.y * ew.bpf + blockIdx.x) * 4, smm);
 }
 
 // p = r + beta (p - omega v)   (only systems that were active in this iteration: flag `upd`)

@@ -111,6 +111,12 @@ struct KSum {
   __device__ __forceinline__ double val() const { return s + c; }
 };
 
+// a plain FP64 running sum with KSum's interface (c stays 0)
+struct PlainSum {
+  double s, c;
+  __device__ __forceinline__ void add(double x) { s += x; }
+};
+
 // Block-wide reduction of K compensated sums; thread 0 writes (s,c) pairs to
 // out[k] (as double2).  smem must hold 2*K*nwarps doubles.
 template <int K>
