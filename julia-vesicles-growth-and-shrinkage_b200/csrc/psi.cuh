@@ -159,6 +159,32 @@ __device__ __forceinline__ double vk_kz2(const VGeom& g, long long s) {
   return kzv * kzv;
 }
 
+// FP32 form of vk + vk_kz2 for the FP32 solve's vector passes: the squared
+// wavenumber |k|^2 (HALF: Nyquist x term zero, as the operator) and the slot
+// weight w.  Integer index arithmetic, FP32 multipliers.
+__device__ __forceinline__ void vk_f32(const VGeom& g, long long s, float& k2, float& w) {
+  const unsigned su = (unsigned)s;
+  int kx, ky;
+  if (g.full) {
+    kx = (int)(su & (unsigned)(g.Nx - 1)); ky = (int)(su >> g.logNx);
+    if (g.nd3) ky &= g.Ny - 1;
+  }
+  else { ky = (int)(su / (unsigned)g.kp); kx = (int)(su - (unsigned)ky * (unsigned)g.kp); }
+  const float kyv = (float)(ky < g.Ny / 2 ? ky : ky - g.Ny) * (float)g.kys;
+  float kxv;
+  if (g.full) { kxv = (float)(kx < g.Nx / 2 ? kx : kx - g.Nx) * (float)g.kxs; w = 1.f; }
+  else {
+    kxv = (kx == g.Nx / 2) ? 0.f : (float)kx * (float)g.kxs;
+    w = (kx >= g.nkx) ? 0.f : ((kx == 0 || kx == g.Nx / 2) ? 1.f : 2.f);
+  }
+  k2 = fmaf(kxv, kxv, kyv * kyv);
+  if (g.nd3) {
+    const int kz = (int)(su >> (g.logNx + g.logNy));
+    const float kzv = (float)(kz < g.Nz / 2 ? kz : kz - g.Nz) * (float)g.kzs;
+    k2 = fmaf(kzv, kzv, k2);
+  }
+}
+
 // y = a_dt * x - ( m_x t1 + i ky t2 ) at slot s of field f (HALF: Nyquist x multiplier zero)
 template <typename T>
 __device__ __forceinline__ double2 op_out(const VGeom& g, const cplx<T>* x, const cplx<T>* t1, const cplx<T>* t2,
@@ -932,6 +958,9 @@ __global__ void __launch_bounds__(256) k_psi_combz(const cplx<T>* __restrict__ x
   block_reduce_store<4>(acc, part + ((long long)f * ew.bpf + blockIdx.x) * 4, smm);
 }
 
+// slots per thread per round of the Krylov vector passes (loads in flight together)
+constexpr int VB = 4;
+
 // r = M^-1 b, x = 0, p = r, dots <b, r>, ||r||^2, ||b||^2  (Krylov.jl bicgstab initialisation)
 template <typename T>
 __global__ void __launch_bounds__(256) k_psi_init(const cplx<T>* __restrict__ b, cplx<T>* __restrict__ x, cplx<T>* __restrict__ r,
@@ -944,30 +973,66 @@ __global__ void __launch_bounds__(256) k_psi_init(const cplx<T>* __restrict__ b,
   const int rr = sm.run_of[f % sm.V];
   const double adt = adt_r[rr], mm = mmax_r ? mmax_r[rr] : 0.0;
   const long long beg = (long long)blockIdx.x * ew.chunk, end = min(ew.n, beg + ew.chunk);
+  if constexpr (std::is_same<T, float>::value) {
+    // FP32 solve: r = M^-1 b in FP32, the dot terms as FP32 products summed over a
+    // round of VB slots, the rounds accumulated in FP64 (as k_psi_update)
+    const float fadt = (float)adt, mms4 = (float)(mm * S4);
+    for (long long qb = beg + threadIdx.x; qb < end; qb += VB * blockDim.x) {
+      float2 bv[VB];
+#pragma unroll
+      for (int u = 0; u < VB; ++u) {
+        const long long q = qb + (long long)u * blockDim.x;
+        if (q < end) bv[u] = b[(long long)f * g.n + q];
+      }
+      float d0 = 0.f, d1 = 0.f, d2 = 0.f, d3 = 0.f;
+#pragma unroll
+      for (int u = 0; u < VB; ++u) {
+        const long long q = qb + (long long)u * blockDim.x;
+        if (q >= end) break;
+        const long long j = (long long)f * g.n + q;
+        float k2, w;
+        vk_f32(g, q, k2, w);
+        const float2 z = make_float2(0.f, 0.f);
+        x[j] = z;
+        if (w == 0.f) { r[j] = z; p[j] = z; continue; }
+        const float pinv = mmax_r ? 1.0f / fmaf(mms4, k2, fadt) : 1.f;
+        const float2 rv = make_float2(bv[u].x * pinv, bv[u].y * pinv);
+        r[j] = rv; p[j] = rv;
+        d0 = fmaf(w, fmaf(bv[u].x, rv.x, bv[u].y * rv.y), d0);
+        d1 += fmaf(bv[u].x, rv.y, -bv[u].y * rv.x);
+        d2 = fmaf(w, fmaf(rv.x, rv.x, rv.y * rv.y), d2);
+        d3 = fmaf(w, fmaf(bv[u].x, bv[u].x, bv[u].y * bv[u].y), d3);
+      }
+      acc[0].add((double)d0);
+      if (g.full) acc[1].add((double)d1);
+      acc[2].add((double)d2);
+      acc[3].add((double)d3);
+    }
+  } else {
 #pragma unroll 4
-  for (long long s = beg + threadIdx.x; s < end; s += blockDim.x) {
-    int kx, ky; double kxv, kyv, w;
-    vk(g, s, kx, ky, kxv, kyv, w);
-    long long j = (long long)f * g.n + s;
-    cplx<T> z{};
-    x[j] = z;
-    if (w == 0.0) { r[j] = z; p[j] = z; continue; }
-    cplx<T> bv = b[j];
-    double kxp = (!g.full && kx == g.Nx / 2) ? 0.0 : kxv;
-    double pinv = mmax_r ? 1.0 / (adt + mm * S4 * (kxp * kxp + kyv * kyv + vk_kz2(g, s))) : 1.0;
-    cplx<T> rv; rv.x = (double)bv.x * pinv; rv.y = (double)bv.y * pinv;
-    r[j] = rv; p[j] = rv;
-    acc[0].add(w * ((double)bv.x * (double)rv.x + (double)bv.y * (double)rv.y));
-    if (g.full) acc[1].add((double)bv.x * (double)rv.y - (double)bv.y * (double)rv.x);
-    acc[2].add(w * ((double)rv.x * (double)rv.x + (double)rv.y * (double)rv.y));
-    acc[3].add(w * ((double)bv.x * (double)bv.x + (double)bv.y * (double)bv.y));   // ||b||^2: the true residual of x0 = 0
+    for (long long s = beg + threadIdx.x; s < end; s += blockDim.x) {
+      int kx, ky; double kxv, kyv, w;
+      vk(g, s, kx, ky, kxv, kyv, w);
+      long long j = (long long)f * g.n + s;
+      cplx<T> z{};
+      x[j] = z;
+      if (w == 0.0) { r[j] = z; p[j] = z; continue; }
+      cplx<T> bv = b[j];
+      double kxp = (!g.full && kx == g.Nx / 2) ? 0.0 : kxv;
+      double pinv = mmax_r ? 1.0 / (adt + mm * S4 * (kxp * kxp + kyv * kyv + vk_kz2(g, s))) : 1.0;
+      cplx<T> rv; rv.x = (double)bv.x * pinv; rv.y = (double)bv.y * pinv;
+      r[j] = rv; p[j] = rv;
+      acc[0].add(w * ((double)bv.x * (double)rv.x + (double)bv.y * (double)rv.y));
+      if (g.full) acc[1].add((double)bv.x * (double)rv.y - (double)bv.y * (double)rv.x);
+      acc[2].add(w * ((double)rv.x * (double)rv.x + (double)rv.y * (double)rv.y));
+      acc[3].add(w * ((double)bv.x * (double)bv.x + (double)bv.y * (double)bv.y));   // ||b||^2: the true residual of x0 = 0
+    }
   }
   block_reduce_store<4>(acc, part + ((long long)blockIdx.y * ew.bpf + blockIdx.x) * 4, smm);
 }
 
 // s = r - alpha v.  Each thread loads VB slots of both operands before it
 // computes, so several loads per thread are in flight.
-constexpr int VB = 4;
 template <typename T>
 __global__ void __launch_bounds__(256) k_psi_s(const cplx<T>* __restrict__ r, const cplx<T>* __restrict__ v,
                                                cplx<T>* __restrict__ s, const BiState* __restrict__ st, SysMap sm, EW ew) {
@@ -1016,7 +1081,62 @@ __global__ void __launch_bounds__(256, 2) k_psi_update(cplx<T>* __restrict__ x, 
   Acc acc[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
   const int f = blockIdx.y;
   const BiState& b = st[sm.sys(f)];
-  if (b.active) {
+  if constexpr (std::is_same<T, float>::value) {
+    // FP32 solve: the updates in FP32 arithmetic (the solve's own precision) and the
+    // dot terms as FP32 products summed over the VB slots of a round, each round's
+    // four partials added in FP64 -- one float-to-double conversion per slot instead
+    // of ~20, which otherwise bound this pass below the copy bandwidth
+    if (b.active) {
+      const float2 al = make_float2((float)b.alpha.x, (float)b.alpha.y);
+      const float2 om = make_float2((float)b.omega.x, (float)b.omega.y);
+      const int run = sm.run_of[f % sm.V];
+      const float adt = mmax_r ? (float)adt_r[run] : 0.f, mms4 = mmax_r ? (float)(mmax_r[run] * S4) : 0.f;
+      const long long base = (long long)f * g.n;
+      const long long beg = (long long)blockIdx.x * ew.chunk, end = min(ew.n, beg + ew.chunk);
+      for (long long qb = beg + threadIdx.x; qb < end; qb += VB * blockDim.x) {
+        float2 xv[VB], pv[VB], sv[VB], tv[VB], hv[VB], cv[VB];
+#pragma unroll
+        for (int u = 0; u < VB; ++u) {
+          const long long q = qb + (long long)u * blockDim.x;
+          if (q < end) {
+            const long long j = base + q;
+            xv[u] = x[j]; pv[u] = p[j]; sv[u] = s[j]; tv[u] = t[j]; cv[u] = cvec[j];
+            hv[u] = shat ? shat[j] : sv[u];
+          }
+        }
+        float d0 = 0.f, d1 = 0.f, d2 = 0.f, d3 = 0.f;
+#pragma unroll
+        for (int u = 0; u < VB; ++u) {
+          const long long q = qb + (long long)u * blockDim.x;
+          if (q >= end) break;
+          float k2, w;
+          vk_f32(g, q, k2, w);
+          if (w == 0.f) continue;
+          const long long j = base + q;
+          float2 xa, xn, rn;
+          xa.x = fmaf(al.x, pv[u].x, fmaf(-al.y, pv[u].y, xv[u].x));
+          xa.y = fmaf(al.x, pv[u].y, fmaf(al.y, pv[u].x, xv[u].y));
+          xn.x = fmaf(om.x, hv[u].x, fmaf(-om.y, hv[u].y, xa.x));
+          xn.y = fmaf(om.x, hv[u].y, fmaf(om.y, hv[u].x, xa.y));
+          x[j] = xn;
+          rn.x = fmaf(-om.x, tv[u].x, fmaf(om.y, tv[u].y, sv[u].x));
+          rn.y = fmaf(-om.x, tv[u].y, fmaf(-om.y, tv[u].x, sv[u].y));
+          r[j] = rn;
+          const float2 c = cv[u];
+          d0 = fmaf(w, fmaf(c.x, rn.x, c.y * rn.y), d0);
+          d1 += fmaf(c.x, rn.y, -c.y * rn.x);
+          const float rr = fmaf(rn.x, rn.x, rn.y * rn.y);
+          d2 = fmaf(w, rr, d2);
+          const float dd = mmax_r ? fmaf(mms4, k2, adt) : 1.f;
+          d3 = fmaf(w * dd, dd * rr, d3);
+        }
+        acc[0].add((double)d0);
+        if (g.full) acc[1].add((double)d1);
+        acc[2].add((double)d2);
+        acc[3].add((double)d3);
+      }
+    }
+  } else if (b.active) {
     const double2 al = b.alpha, om = b.omega;
     const int run = sm.run_of[f % sm.V];
     const double adt = mmax_r ? adt_r[run] : 0.0, mm = mmax_r ? mmax_r[run] : 0.0;
