@@ -448,7 +448,10 @@ __global__ void __launch_bounds__(NT, MinB<E, NT>::v) k_psi_cols_comb(const cplx
 // Shared memory (dynamic, 1024-byte aligned):
 //   staging  A arrays x [L][TW] (TMA box layout), A = 1 (inv2) or 4 (comb: t1 t2 x c)
 //   work     col_tile_elems(L, 2 TW, log2 E) complex (the FFT buffer)
-//   2 mbarriers
+//   2 mbarriers (64 bytes)
+//   twx      the last FFT pass's per-butterfly twiddles (tw_last_table), staged once
+//            per block, so that pass reads consecutive shared words instead of
+//            strided entries of the global table
 // ---------------------------------------------------------------------------
 struct TmaTiles {
   int total;        // tiles over the chunk's fields: fc * tiles
@@ -462,8 +465,12 @@ __host__ __device__ __forceinline__ size_t tma_col_smem(int L, int TW, int E, in
   int loge = 0;
   while ((1 << loge) < E) ++loge;
   const size_t work = (size_t)col_tile_elems(L, 2 * TW, loge) * sizeof(float2);
-  return 1024 + stage + work + 64;
+  const size_t twx = (size_t)(E >= 16 ? 3 + E / 4 - 1 : E - 1) * (L / E) * sizeof(float2);
+  return 1024 + stage + work + 64 + twx;
 }
+
+// the last-pass twiddle table (tw_last_table) of a TMA column pass, after its mbarriers
+__device__ __forceinline__ float2* tma_twx(uint64_t* bar) { return reinterpret_cast<float2*>(reinterpret_cast<unsigned char*>(bar) + 64); }
 
 __device__ __forceinline__ unsigned char* tma_smem_base() {
   extern __shared__ __align__(16) unsigned char smraw_tma[];
@@ -499,7 +506,9 @@ __global__ void __launch_bounds__(NT, NT <= 512 ? 2 : 1) k_psi_cols_inv2_tma(con
     mbar_arrive_expect_tx(bar, tx);
     for (int q = 0; q < NBOX; ++q) tma_load_2d(sx + (size_t)q * BH * TW, &mx, c0, (f0 + fl) * a.Ny + q * BH, bar);
   };
+  C* twx = tma_twx(bar);
   if (tid == 0) { mbar_init(bar, 1); mbar_fence_init(); }
+  tw_last_table<E>(twx, LOGL, tab);
   __syncthreads();
   int t = next(blockIdx.x);
   if (tid == 0 && t < tt.total) issue(t);
@@ -526,7 +535,7 @@ __global__ void __launch_bounds__(NT, NT <= 512 ? 2 : 1) k_psi_cols_inv2_tma(con
     __syncthreads();                                          // staging consumed by every thread
     const int tn = next(t + gridDim.x);
     if (tid == 0 && tn < tt.total) { fence_proxy_async(); issue(tn); }
-    tile_fft_1buf<E, true>(v, work, lay, line, i, LOGL, lognl, tab);
+    tile_fft_1buf<E, true>(v, work, lay, line, i, LOGL, lognl, tab, twx);
     C* o = (dir_y ? t2 : t1) + (long long)fl * a.O + c;
 #pragma unroll
     for (int j = 0; j < E; ++j) o[(long long)(i + j * LE) * a.S] = v[j];
@@ -587,7 +596,9 @@ __global__ void __launch_bounds__(NT, E * NT <= 4096 ? 2 : 1) k_psi_cols_comb_tm
       tma_load_2d(scv + (size_t)q * BH * TW, &mc, c0, (f0 + fl) * a.Ny + q * BH, &bar[1]);
     }
   };
+  C* twx = tma_twx(bar);
   if (tid == 0) { mbar_init(&bar[0], 1); mbar_init(&bar[1], 1); mbar_fence_init(); }
+  tw_last_table<E>(twx, LOGL, tab);
   __syncthreads();
   // tiles of inactive systems get zero dot partials (the per-tile layout of k_psi_cols_comb)
   for (int t = blockIdx.x; t < tt.total; t += gridDim.x)
@@ -607,7 +618,7 @@ __global__ void __launch_bounds__(NT, E * NT <= 4096 ? 2 : 1) k_psi_cols_comb_tm
     __syncthreads();                                          // t1 / t2 staging consumed
     const int tn = next(t + gridDim.x);
     if (tid == 0 && tn < tt.total) { fence_proxy_async(); issue_t(tn); }
-    tile_fft_1buf<E, false>(v, work, lay, line, i, LOGL, lognl, tab);
+    tile_fft_1buf<E, false>(v, work, lay, line, i, LOGL, lognl, tab, twx);
     // trade halves with the partner TW lanes away: the t1 holder keeps rows j < E/2,
     // the t2 holder rows j >= E/2
     constexpr int H = E / 2;
