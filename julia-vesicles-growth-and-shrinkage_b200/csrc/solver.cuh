@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <mutex>
 #include "psi.cuh"
+#include "cols_tma.cuh"
 #include "net_apply.cuh"
 #include "net_tc.cuh"
 
@@ -551,6 +552,18 @@ class Solver : public SolverBase {
     // forward pass + combine; read once here, so it holds for this handle's whole life
     // (graph replays included) and is what the tuning record reports
     if (const char* env = getenv("VSAV_PSI_SPLIT")) split_comb = atoi(env) != 0;
+    // VSAV_COLS_TMA overrides the choice of the TMA-fed field column pass (where eligible):
+    // 0 off, 1 on (the tuned block shape, else the first usable one), 2 + v block shape v
+    if (const char* env = getenv("VSAV_COLS_TMA")) {
+      const int b = atoi(env);
+      if (b >= 2) { cols_tma_var = b - 2; cols_tma = cols_tma_var_ok(cols_tma_var); }
+      else {
+        cols_tma = b != 0 && cols_tma_eligible();
+        for (int v = CT_NV - 1; cols_tma && v >= 0; --v)
+          if (!cols_tma_var_ok(cols_tma_var)) cols_tma_var = v;
+      }
+      if (!cols_tma) cols_tma_var = 0;
+    }
     // VSAV_PSI_TMA=0/1 overrides the choice of the TMA-fed psi column passes (where eligible)
     if (const char* env = getenv("VSAV_PSI_TMA")) {
       tma_cols = atoi(env) != 0 && tma_eligible();
@@ -744,6 +757,10 @@ class Solver : public SolverBase {
   }
   void cols(bool inv, int geo, long long nf, const C* in0, const C* in1, double a0, double a1, int mult, double ms,
             C* out, double oscale) {
+    if (cols_tma && geo == 0 && g.nd == 2) {
+      cols_tma_run(inv, nf, in0, in1, a0, a1, mult, ms, out, oscale, cols_tma_var);
+      return;
+    }
     VSAV_DISPATCH(geo == 3 ? FAM_COLS_PSI : FAM_COLS, {
       long long nouter = nf;
       ColArgs a = colargs(geo, nouter, E_, NT_);
@@ -930,6 +947,92 @@ class Solver : public SolverBase {
   // L = 1024, one block per SM for the combine), variant 1 E 8 / NT 512 (tiles of 4096:
   // 2 columns, two blocks per SM); the autotuner picks one per pass.  Column lengths
   // L = 256 .. 2048 are compiled (tma_var_ok).
+  // ---- the TMA-fed persistent y pass of the 2D half-spectrum field transforms
+  // (k_cols_tma, cols_tma.cuh): two block shapes, both with 2-column tiles at
+  // L = 1024 (E 16 / NT 128: three blocks per SM in FP64; E 8 / NT 256), column
+  // lengths L = 256 .. 2048; autotuned against k_cols (the classic family FAM_COLS)
+  static constexpr int CT_NV = 2;
+  static constexpr int CT_E[CT_NV] = {16, 8}, CT_NT[CT_NV] = {128, 256};
+  int cols_tma = 0, cols_tma_var = 0;
+  double cols_tma_ms[CT_NV] = {0.0, 0.0};
+  int cols_tma_ctas[2][2][CT_NV] = {};           // [inverse][inputs - 1][variant] resident blocks
+  bool cols_tma_var_ok(int v) const {
+    if (v < 0 || v >= CT_NV) return false;
+    const int L = g.Ny, E = CT_E[v], TW = CT_E[v] * CT_NT[v] / L;
+    return g.nd == 2 && L >= 256 && L <= 2048 && L >= E * E && TW >= 2 && TW <= 16 && g.kp % TW == 0;
+  }
+  bool cols_tma_eligible() const {
+    for (int v = 0; v < CT_NV; ++v)
+      if (cols_tma_var_ok(v)) return true;
+    return false;
+  }
+  template <int E_, int NT_, int LOGL>
+  static constexpr bool cols_tma_shape_ok() {
+    constexpr int L = 1 << LOGL, TW = E_ * NT_ / L;
+    return TW >= 2 && TW <= 16 && L >= E_ * E_;
+  }
+  // tensor map of nouter * Ny half-spectrum rows of kp complex values
+  const CUtensorMap* tmap_half(const C* base, long long rows, int TW, int BH) {
+    auto key = std::make_pair((const void*)base, -(rows * 4096 + TW * 512 + BH));
+    auto it = tmaps.find(key);
+    if (it == tmaps.end()) it = tmaps.emplace(key, make_tile_map(base, (int)sizeof(C), rows, g.kp, TW, BH)).first;
+    return &it->second;
+  }
+  template <int E_, int NT_, int LOGL, bool INV, int NIN>
+  void launch_cols_tma(long long nouter, const C* in0, const C* in1, double a0, double a1, int mult, double ms, C* out,
+                       double oscale, int var) {
+    constexpr int L = 1 << LOGL, TW = E_ * NT_ / L, BH = L < 256 ? L : 256;
+    long long no = nouter;
+    ColArgs a = colargs(0, no, E_, NT_);
+    if (a.TW != TW) throw std::runtime_error("TMA field column pass: tile width mismatch");
+    ColsTmaTiles tt;
+    tt.per_field = (g.nkx + TW - 1) / TW;
+    tt.total = (int)(tt.per_field * nouter);
+    const size_t smem = cols_tma_smem<T, E_, NT_, LOGL, NIN>();
+    const CUtensorMap* m0 = tmap_half(in0, nouter * g.Ny, TW, BH);
+    const CUtensorMap* m1 = NIN == 2 ? tmap_half(in1, nouter * g.Ny, TW, BH) : m0;
+    const void* fn = (const void*)k_cols_tma<T, E_, NT_, LOGL, INV, NIN>;
+    const int grid = std::min(tt.total, tma_grid(fn, NT_, smem, cols_tma_ctas[INV ? 1 : 0][NIN - 1][var]));
+    prof.begin(st);
+    k_cols_tma<T, E_, NT_, LOGL, INV, NIN><<<grid, NT_, smem, st>>>(*m0, *m1, (T)a0, (T)a1, mult, ms, out, (T)oscale, a, tt,
+                                                                    tab, d_err);
+    VSAV_COUNT_LAUNCH();
+    VSAV_LAUNCH_CHECK();
+    prof.end(st, std::is_same<T, float>::value ? KC_COLS_F32 : KC_COLS,
+             (double)nouter * g.nkx * L * sizeof(C) * (NIN + 1));
+  }
+  template <int LOGL, bool INV, int NIN>
+  void cols_tma_L(long long nf, const C* in0, const C* in1, double a0, double a1, int mult, double ms, C* out,
+                  double oscale, int var) {
+    if constexpr (cols_tma_shape_ok<CT_E[0], CT_NT[0], LOGL>())
+      if (var == 0) { launch_cols_tma<CT_E[0], CT_NT[0], LOGL, INV, NIN>(nf, in0, in1, a0, a1, mult, ms, out, oscale, 0); return; }
+    if constexpr (cols_tma_shape_ok<CT_E[1], CT_NT[1], LOGL>())
+      if (var == 1) { launch_cols_tma<CT_E[1], CT_NT[1], LOGL, INV, NIN>(nf, in0, in1, a0, a1, mult, ms, out, oscale, 1); return; }
+    throw std::runtime_error("TMA field column pass: block shape not compiled for this column length");
+  }
+  template <int LOGL>
+  void cols_tma_I(bool inv, long long nf, const C* in0, const C* in1, double a0, double a1, int mult, double ms, C* out,
+                  double oscale, int var) {
+    if (inv) {
+      if (in1) cols_tma_L<LOGL, true, 2>(nf, in0, in1, a0, a1, mult, ms, out, oscale, var);
+      else cols_tma_L<LOGL, true, 1>(nf, in0, in1, a0, a1, mult, ms, out, oscale, var);
+    } else {
+      if (in1) cols_tma_L<LOGL, false, 2>(nf, in0, in1, a0, a1, mult, ms, out, oscale, var);
+      else cols_tma_L<LOGL, false, 1>(nf, in0, in1, a0, a1, mult, ms, out, oscale, var);
+    }
+  }
+  void cols_tma_run(bool inv, long long nf, const C* in0, const C* in1, double a0, double a1, int mult, double ms, C* out,
+                    double oscale, int var) {
+    if (!cols_tma_var_ok(var)) throw std::runtime_error("TMA field column pass: block shape unusable at this size");
+    switch (ilog2(g.Ny)) {
+      case 8: cols_tma_I<8>(inv, nf, in0, in1, a0, a1, mult, ms, out, oscale, var); break;
+      case 9: cols_tma_I<9>(inv, nf, in0, in1, a0, a1, mult, ms, out, oscale, var); break;
+      case 10: cols_tma_I<10>(inv, nf, in0, in1, a0, a1, mult, ms, out, oscale, var); break;
+      case 11: cols_tma_I<11>(inv, nf, in0, in1, a0, a1, mult, ms, out, oscale, var); break;
+      default: throw std::runtime_error("TMA field column pass: unsupported column length");
+    }
+  }
+
   static constexpr int TMA_NV = 2;
   static constexpr int TMA_VE[TMA_NV] = {16, 8}, TMA_VNT[TMA_NV] = {512, 512};
   int tma_cols = 0;               // 1: the psi column passes run as the TMA-fed kernels (autotuned)
@@ -1179,7 +1282,8 @@ class Solver : public SolverBase {
     std::lock_guard<std::mutex> lk(tune_mutex());
     std::vector<int> c(choice, choice + FAM_N);
     c.push_back(split_comb);
-    c.push_back(tma_cols | tma_var_inv2 << 1 | tma_var_comb << 3 | bulk_rows << 5 | bulk_var << 6);
+    c.push_back(tma_cols | tma_var_inv2 << 1 | tma_var_comb << 3 | bulk_rows << 5 | bulk_var << 6 | cols_tma << 8 |
+                cols_tma_var << 9);
     tune_cache()[tune_key()] = c;
     if (tfile && *tfile) {
       std::map<std::string, std::vector<int>> fm;
@@ -1196,6 +1300,9 @@ class Solver : public SolverBase {
     bulk_var = (code >> 6) & 3;
     bulk_rows = ((code >> 5) & 1) && bulk_eligible() && bulk_var_ok(bulk_var);
     if (!bulk_rows) bulk_var = 0;
+    cols_tma_var = (code >> 9) & 1;
+    cols_tma = ((code >> 8) & 1) && cols_tma_var_ok(cols_tma_var);
+    if (!cols_tma) cols_tma_var = 0;
   }
   // the variants in use, as JSON: {"key", "source", "split", families: "E<e>/NT<nt>"}
   std::string tuning_json() const {
@@ -1203,7 +1310,9 @@ class Solver : public SolverBase {
                                     "psi_comb", "psi_fwd2"};
     std::string o = "{\"key\": \"" + tune_key() + "\", \"source\": \"" + tune_source + "\", \"psi_forward_combine\": \"" +
                     (split_comb ? "split" : "fused") + "\", \"psi_column_passes\": \"" +
-                    (tma_cols ? "tma" : "classic") + "\", \"variants\": {";
+                    (tma_cols ? "tma" : "classic") + "\", \"field_column_pass\": \"" +
+                    (cols_tma ? "tma E" + std::to_string(CT_E[cols_tma_var]) + "/NT" + std::to_string(CT_NT[cols_tma_var])
+                              : std::string("classic")) + "\", \"variants\": {";
     o += std::string("\"psi_rows\": \"") +
          (bulk_rows ? "bulk E" + std::to_string(BR_E[bulk_var]) + "/NT" + std::to_string(BR_NT[bulk_var]) + "/S" +
                           std::to_string(BR_S[bulk_var])
@@ -1233,6 +1342,7 @@ class Solver : public SolverBase {
     bool have_mul = (g.nd == 2) && vt12 != nullptr;
     // the fused x pass skips inactive systems: time it with every system active
     if (have_mul) VSAV_CUDA(cudaMemsetAsync(bupd, 0xff, 3 * dm.R * sizeof(int), st));
+    cols_tma = 0;
     for (int fam = 0; fam < FAM_N; ++fam) {
       if (fam == FAM_MUL && !have_mul) continue;
       if ((fam == FAM_C2C || fam == FAM_COLS_PSI || fam == FAM_PSI_INV2 || fam == FAM_PSI_COMB || fam == FAM_PSI_FWD2) &&
@@ -1268,6 +1378,25 @@ class Solver : public SolverBase {
         if (ms < best) { best = ms; bestv = v; }
       }
       choice[fam] = bestv;
+    }
+    // the TMA-fed field column pass against the classic one (as chosen above), on the same call
+    if (cols_tma_eligible()) {
+      double best = 1e30;
+      int bv = -1;
+      for (int v = 0; v < CT_NV; ++v) {
+        if (!cols_tma_var_ok(v)) continue;
+        auto fn = [&]() { cols_tma_run(false, V, tmpH, nullptr, 1, 0, M_ONE, 1, tmpH, 1, v); };
+        fn();
+        VSAV_CUDA(cudaEventRecord(e0, st));
+        for (int k = 0; k < 3; ++k) fn();
+        VSAV_CUDA(cudaEventRecord(e1, st));
+        VSAV_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        VSAV_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        cols_tma_ms[v] = ms / 3;
+        if (cols_tma_ms[v] < best) { best = cols_tma_ms[v]; bv = v; }
+      }
+      if (bv >= 0 && best < tune_ms[FAM_COLS][choice[FAM_COLS]]) { cols_tma = 1; cols_tma_var = bv; }
     }
     // split or fused forward pass + combine: the split pair's streaming combine timed on the same fields
     split_comb = 0;

@@ -5,7 +5,9 @@ instead of CUDA-graph replay (VSAV_GRAPH=0), and either form of the operator's
 forward pass (VSAV_PSI_SPLIT=1: k_psi_cols_fwd2 + k_psi_combz; 0: the fused
 k_psi_cols_comb), whichever the autotuner picked, and the operator's x pass as
 the classic kernel (VSAV_PSI_BULK=0) or as each block shape of the bulk-copy-fed
-persistent kernel (VSAV_PSI_BULK=2, 3, 4; FP32 psi solves only)."""
+persistent kernel (VSAV_PSI_BULK=2, 3, 4; FP32 psi solves only), and the y pass of
+the field transforms as the classic kernel (VSAV_COLS_TMA=0) or as each block
+shape of the TMA-fed persistent kernel (VSAV_COLS_TMA=2, 3)."""
 import numpy as np
 import pytest
 
@@ -31,7 +33,8 @@ def run(kw, phi, psi, prec, steps=3):
 @pytest.mark.parametrize("prec", ["fp64", "mixed", "fp32"])
 @pytest.mark.parametrize("env", [("VSAV_PSI_FUSED", "0"), ("VSAV_PSI_CHUNK_MB", "1"), ("VSAV_GRAPH", "0"),
                                  ("VSAV_PSI_SPLIT", "1"), ("VSAV_PSI_SPLIT", "0"), ("VSAV_PSI_BULK", "0"),
-                                 ("VSAV_PSI_BULK", "2"), ("VSAV_PSI_BULK", "3"), ("VSAV_PSI_BULK", "4")])
+                                 ("VSAV_PSI_BULK", "2"), ("VSAV_PSI_BULK", "3"), ("VSAV_PSI_BULK", "4"),
+                                 ("VSAV_COLS_TMA", "0"), ("VSAV_COLS_TMA", "2"), ("VSAV_COLS_TMA", "3")])
 def test_switches_keep_the_results(prec, env, monkeypatch):
     from vsav import ics
     kw, phi, psi, _ = ics.workload("multi2d_512x4", seed=2, n_override=256, N_override=2, eps_override=0.08)
@@ -68,3 +71,24 @@ def test_bulk_x_pass_block_shapes(n, shape, monkeypatch):
     for k in FIELDS:
         assert rel(alt[k], base[k]) < 1e-10, (k, rel(alt[k], base[k]))
     np.testing.assert_allclose(alt["E"], base["E"], rtol=1e-10)
+
+
+@pytest.mark.parametrize("n", [256, 512, 1024])
+@pytest.mark.parametrize("shape", ["2", "3"])
+def test_field_column_tma_block_shapes(n, shape, monkeypatch):
+    """Both block shapes of the TMA-fed y pass of the field transforms at the column
+    lengths 256, 512 and 1024 give the classic kernel's results on the FP64 parity
+    path (every field transform of Steps 1-7 and the state update runs through it).
+    The classic variant the autotuner picks may split the radix differently, so the
+    fields agree up to rounding order, which the velocity amplifies (1e-10 bar)."""
+    from vsav import ics
+    kw, phi, psi, _ = ics.workload("multi2d_512x4", seed=4, n_override=n, N_override=2, eps_override=0.08)
+    kw["dt"] = 1e-6
+    monkeypatch.setenv("VSAV_COLS_TMA", "0")
+    base = run(kw, phi, psi, "fp64", steps=2)
+    monkeypatch.setenv("VSAV_COLS_TMA", shape)
+    alt = run(kw, phi, psi, "fp64", steps=2)
+    for k in FIELDS:
+        assert rel(alt[k], base[k]) < 1e-10, (k, rel(alt[k], base[k]))
+    np.testing.assert_allclose(alt["E"], base["E"], rtol=1e-10)
+    assert np.array_equal(alt["iters"], base["iters"])
