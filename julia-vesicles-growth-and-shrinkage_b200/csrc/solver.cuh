@@ -18,6 +18,7 @@
 #include <mutex>
 #include "psi.cuh"
 #include "cols_tma.cuh"
+#include "c2r_bulk.cuh"
 #include "net_apply.cuh"
 #include "net_tc.cuh"
 
@@ -564,6 +565,8 @@ class Solver : public SolverBase {
       }
       if (!cols_tma) cols_tma_var = 0;
     }
+    // VSAV_C2R_BULK=0/1 overrides the choice of the bulk-copy-fed c2r x pass (where eligible)
+    if (const char* env = getenv("VSAV_C2R_BULK")) c2r_bulk = atoi(env) != 0 && c2r_bulk_shape();
     // VSAV_PSI_TMA=0/1 overrides the choice of the TMA-fed psi column passes (where eligible)
     if (const char* env = getenv("VSAV_PSI_TMA")) {
       tma_cols = atoi(env) != 0 && tma_eligible();
@@ -704,6 +707,7 @@ class Solver : public SolverBase {
     })
   }
   void rows_c2r(const C* in, T* out, double scale, long long nrows) {
+    if (c2r_bulk && c2r_bulk_ok(nrows)) { rows_c2r_bulk(in, out, scale, nrows); return; }
     int L = g.Nx / 2, logL = ilog2(L);
     VSAV_DISPATCH(FAM_C2R, {
       int lognl = rows_lognl(L, E_, NT_, nrows);
@@ -717,6 +721,39 @@ class Solver : public SolverBase {
       VSAV_LAUNCH_CHECK();
       prof.end(st, KC_ROWS_C2R, (double)nrows * (g.Nx * sizeof(T) + g.nkx * sizeof(C)));
     })
+  }
+  // ---- the bulk-copy-fed c2r x pass (k_rows_c2r_bulk, c2r_bulk.cuh): E 8 / 256 threads,
+  // half-length rows L = Nx/2 = 256 .. 1024; autotuned against k_rows_c2r (FAM_C2R)
+  static constexpr int CB_E = 8, CB_NT = 256;
+  int c2r_bulk = 0;
+  double c2r_bulk_ms = 0.0;
+  int c2r_bulk_ctas = 0;
+  bool c2r_bulk_shape() const {
+    const int L = g.Nx / 2;
+    return L >= 256 && L <= 1024 && L >= CB_E * CB_E && CB_E * CB_NT / L >= 1;
+  }
+  bool c2r_bulk_ok(long long nrows) const { return c2r_bulk_shape() && nrows % (CB_E * CB_NT / (g.Nx / 2)) == 0; }
+  template <int LOGL>
+  void launch_c2r_bulk(const C* in, T* out, double scale, long long nrows) {
+    constexpr int L = 1 << LOGL, NL = CB_E * CB_NT / L;
+    const long long nb = nrows / NL;
+    const size_t smem = c2r_bulk_smem<T, CB_E, CB_NT, LOGL>(g.kp);
+    const void* fn = (const void*)k_rows_c2r_bulk<T, CB_E, CB_NT, LOGL>;
+    const int grid = (int)std::min<long long>(nb, tma_grid(fn, CB_NT, smem, c2r_bulk_ctas));
+    prof.begin(st);
+    k_rows_c2r_bulk<T, CB_E, CB_NT, LOGL><<<grid, CB_NT, smem, st>>>(in, out, (T)scale, nb, g.kp, tab, d_err);
+    VSAV_COUNT_LAUNCH();
+    VSAV_LAUNCH_CHECK();
+    prof.end(st, KC_ROWS_C2R, (double)nrows * (g.Nx * sizeof(T) + g.nkx * sizeof(C)));
+  }
+  void rows_c2r_bulk(const C* in, T* out, double scale, long long nrows) {
+    if (!c2r_bulk_ok(nrows)) throw std::runtime_error("bulk c2r pass: unusable row count or length");
+    switch (ilog2(g.Nx / 2)) {
+      case 8: launch_c2r_bulk<8>(in, out, scale, nrows); break;
+      case 9: launch_c2r_bulk<9>(in, out, scale, nrows); break;
+      case 10: launch_c2r_bulk<10>(in, out, scale, nrows); break;
+      default: throw std::runtime_error("bulk c2r pass: unsupported row length");
+    }
   }
   template <bool INV>
   void rows_c2c(const C* in, const T* in_real, C* out, double scale, long long nrows) {
@@ -1283,7 +1320,7 @@ class Solver : public SolverBase {
     std::vector<int> c(choice, choice + FAM_N);
     c.push_back(split_comb);
     c.push_back(tma_cols | tma_var_inv2 << 1 | tma_var_comb << 3 | bulk_rows << 5 | bulk_var << 6 | cols_tma << 8 |
-                cols_tma_var << 9);
+                cols_tma_var << 9 | c2r_bulk << 10);
     tune_cache()[tune_key()] = c;
     if (tfile && *tfile) {
       std::map<std::string, std::vector<int>> fm;
@@ -1303,6 +1340,7 @@ class Solver : public SolverBase {
     cols_tma_var = (code >> 9) & 1;
     cols_tma = ((code >> 8) & 1) && cols_tma_var_ok(cols_tma_var);
     if (!cols_tma) cols_tma_var = 0;
+    c2r_bulk = ((code >> 10) & 1) && c2r_bulk_shape();
   }
   // the variants in use, as JSON: {"key", "source", "split", families: "E<e>/NT<nt>"}
   std::string tuning_json() const {
@@ -1312,7 +1350,9 @@ class Solver : public SolverBase {
                     (split_comb ? "split" : "fused") + "\", \"psi_column_passes\": \"" +
                     (tma_cols ? "tma" : "classic") + "\", \"field_column_pass\": \"" +
                     (cols_tma ? "tma E" + std::to_string(CT_E[cols_tma_var]) + "/NT" + std::to_string(CT_NT[cols_tma_var])
-                              : std::string("classic")) + "\", \"variants\": {";
+                              : std::string("classic")) + "\", \"field_c2r_pass\": \"" +
+                    (c2r_bulk ? "bulk E" + std::to_string(CB_E) + "/NT" + std::to_string(CB_NT) : std::string("classic")) +
+                    "\", \"variants\": {";
     o += std::string("\"psi_rows\": \"") +
          (bulk_rows ? "bulk E" + std::to_string(BR_E[bulk_var]) + "/NT" + std::to_string(BR_NT[bulk_var]) + "/S" +
                           std::to_string(BR_S[bulk_var])
@@ -1343,6 +1383,7 @@ class Solver : public SolverBase {
     // the fused x pass skips inactive systems: time it with every system active
     if (have_mul) VSAV_CUDA(cudaMemsetAsync(bupd, 0xff, 3 * dm.R * sizeof(int), st));
     cols_tma = 0;
+    c2r_bulk = 0;
     for (int fam = 0; fam < FAM_N; ++fam) {
       if (fam == FAM_MUL && !have_mul) continue;
       if ((fam == FAM_C2C || fam == FAM_COLS_PSI || fam == FAM_PSI_INV2 || fam == FAM_PSI_COMB || fam == FAM_PSI_FWD2) &&
@@ -1378,6 +1419,19 @@ class Solver : public SolverBase {
         if (ms < best) { best = ms; bestv = v; }
       }
       choice[fam] = bestv;
+    }
+    // the bulk-copy-fed c2r x pass against the classic one (as chosen above), on the same call
+    if (c2r_bulk_ok(nrows)) {
+      auto fn = [&]() { rows_c2r_bulk(tmpH, tmpP, 1.0, nrows); };
+      fn();
+      VSAV_CUDA(cudaEventRecord(e0, st));
+      for (int k = 0; k < 3; ++k) fn();
+      VSAV_CUDA(cudaEventRecord(e1, st));
+      VSAV_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      VSAV_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      c2r_bulk_ms = ms / 3;
+      c2r_bulk = c2r_bulk_ms < tune_ms[FAM_C2R][choice[FAM_C2R]];
     }
     // the TMA-fed field column pass against the classic one (as chosen above), on the same call
     if (cols_tma_eligible()) {

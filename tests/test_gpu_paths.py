@@ -7,7 +7,8 @@ k_psi_cols_comb), whichever the autotuner picked, and the operator's x pass as
 the classic kernel (VSAV_PSI_BULK=0) or as each block shape of the bulk-copy-fed
 persistent kernel (VSAV_PSI_BULK=2, 3, 4; FP32 psi solves only), and the y pass of
 the field transforms as the classic kernel (VSAV_COLS_TMA=0) or as each block
-shape of the TMA-fed persistent kernel (VSAV_COLS_TMA=2, 3)."""
+shape of the TMA-fed persistent kernel (VSAV_COLS_TMA=2, 3), and their c2r x pass
+as the classic kernel or the bulk-copy-fed persistent one (VSAV_C2R_BULK=0, 1)."""
 import numpy as np
 import pytest
 
@@ -88,6 +89,27 @@ def test_field_column_tma_block_shapes(n, shape, monkeypatch):
     base = run(kw, phi, psi, "fp64", steps=2)
     monkeypatch.setenv("VSAV_COLS_TMA", shape)
     alt = run(kw, phi, psi, "fp64", steps=2)
+    for k in FIELDS:
+        assert rel(alt[k], base[k]) < 1e-10, (k, rel(alt[k], base[k]))
+    np.testing.assert_allclose(alt["E"], base["E"], rtol=1e-10)
+    assert np.array_equal(alt["iters"], base["iters"])
+
+
+@pytest.mark.parametrize("n", [512, 1024, 2048])
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_c2r_bulk_pass(n, prec, monkeypatch):
+    """The bulk-copy-fed c2r x pass at the row lengths 512, 1024 and 2048 (half-length
+    transforms of 256, 512 and 1024 points) gives the classic kernel's results: every
+    half-spectrum to real field transform of Steps 1-7 and the state update runs
+    through it.  The classic variant the autotuner picks may split the radix
+    differently, so the bar is rounding order amplified by the velocity (1e-10)."""
+    from vsav import ics
+    kw, phi, psi, _ = ics.workload("multi2d_512x4", seed=5, n_override=n, N_override=1, eps_override=0.08)
+    kw["dt"] = 1e-6
+    monkeypatch.setenv("VSAV_C2R_BULK", "0")
+    base = run(kw, phi, psi, prec, steps=2)
+    monkeypatch.setenv("VSAV_C2R_BULK", "1")
+    alt = run(kw, phi, psi, prec, steps=2)
     for k in FIELDS:
         assert rel(alt[k], base[k]) < 1e-10, (k, rel(alt[k], base[k]))
     np.testing.assert_allclose(alt["E"], base["E"], rtol=1e-10)
