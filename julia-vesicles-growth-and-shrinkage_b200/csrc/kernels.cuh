@@ -396,9 +396,9 @@ __global__ void k_nu(cplx<T>* __restrict__ cache, const cplx<T>* __restrict__ Gh
 // (phi11 phi12 phi13 phi14 phi21 psi11 psi12 psi21); H4 = [H1|H2|H3|G]
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256) k_dot2(const T* __restrict__ H4, const T* __restrict__ phi, const T* __restrict__ phio,
-                                              const T* __restrict__ psi, const T* __restrict__ psio, const T* __restrict__ cp,
-                                              double b, double c, long long VP, EW ew, double2* part) {
+__global__ void __launch_bounds__(256, 2) k_dot2(const T* __restrict__ H4, const T* __restrict__ phi, const T* __restrict__ phio,
+                                                 const T* __restrict__ psi, const T* __restrict__ psio, const T* __restrict__ cp,
+                                                 double b, double c, long long VP, EW ew, double2* part) {
   __shared__ double sm[2 * 22 * 8];
   KSum acc[22];
 #pragma unroll
